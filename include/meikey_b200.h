@@ -1,0 +1,158 @@
+/*
+ * meikey_b200 — C ABI of the B200 (sm_100a) candidate-key search backend.
+ *
+ * Drop-in boundary for meikey's GPU search backend: the calls below take the place
+ * of the reference's `Engine` trait and `Kernel` (src/service/gpu.rs:806-887), which
+ * the `Gpu` searcher (src/service/gpu.rs:1162-1327) drives from one host thread per
+ * device.  All entry points return an `int` status (MK_OK = 0) and never abort the
+ * process; the text of the last error of a context is kept in that context.
+ * Plain pointers and sizes only: every buffer named "host" is ordinary host memory,
+ * read or written only during the call.
+ *
+ * Seeds (src/model/search.rs:27-50, src/service/gpu.rs:1330-1351):
+ *   MK_SEED_CHACHA20  seed(i) = 32-byte half (i & 1) of ChaCha20 block i >> 1
+ *                     (RFC 8439 block function, 64-bit counter, stream 0), key = `key`
+ *   MK_SEED_COUNTER   seed(i) = key with i added to its last 8 bytes (little-endian)
+ * The public key of a seed is the Ed25519 public key: compress(clamp(SHA-512(seed)[0..32])·B).
+ */
+#ifndef MEIKEY_B200_H
+#define MEIKEY_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MK_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define MK_API __attribute__((visibility("default")))
+#else
+#define MK_API
+#endif
+
+/* Status codes.  1..8 mirror the reference's GpuError (src/service/gpu.rs:444-499);
+ * the rest are states the reference reported by panicking or not at all. */
+enum mk_status {
+    MK_OK = 0,
+    MK_ERR_DRIVER_NOT_FOUND = 1, /* GpuError::DriverNotFound */
+    MK_ERR_NO_DEVICE = 2,        /* GpuError::NoDevice */
+    MK_ERR_OUT_OF_RANGE = 3,     /* GpuError::OutOfRange: an option outside its range */
+    MK_ERR_SELF_CHECK = 4,       /* GpuError::SelfCheck: GPU keys differ from the host derivation */
+    MK_ERR_NO_SETTINGS = 5,      /* GpuError::NoSettings: autotuner had nothing to measure */
+    MK_ERR_CUDA = 6,             /* GpuError::Driver: a CUDA runtime call failed */
+    MK_ERR_NOT_BUILT = 7,        /* GpuError::NotEmbedded: no kernel variant for these options */
+    MK_ERR_BAD_ARG = 8,          /* null pointer, bad mode, needle too long, ... */
+    MK_ERR_OUT_OF_MEMORY = 9,
+    MK_ERR_STOPPED = 10,         /* the launch ended early on the job's stop word */
+    MK_ERR_HIT_RING_FULL = 11,   /* more hits than the hit ring holds; hits beyond it are counted only */
+    MK_ERR_PATTERN = 12          /* pattern text rejected (src/model/pattern.rs:21-52) */
+};
+
+/* seed sources (SeedSource, src/model/search.rs:27-36) */
+enum mk_seed_source { MK_SEED_CHACHA20 = 0, MK_SEED_COUNTER = 1 };
+
+/* match modes (kernel.cu MODE_CONTAINS / MODE_SUFFIX / MODE_REGEX, src/service/gpu.rs:610-616) */
+enum mk_mode { MK_MODE_CONTAINS = 0, MK_MODE_SUFFIX = 1, MK_MODE_REGEX = 2 };
+
+/* Kernel options (GpuOptions, src/service/gpu.rs:189-199).  Zero means "default".
+ * table_rows chooses the comb geometry (rows of the fixed-base table: fewer rows
+ * means fewer point additions per key and a larger table in HBM). */
+typedef struct mk_options {
+    uint32_t table_rows;      /* 10..16; default 12 */
+    uint32_t keys_per_thread; /* keys one thread derives before the pooled inversion: 4, 8 or 16 */
+    uint32_t block;           /* threads per CTA: 128 or 256 */
+    uint32_t blocks_per_sm;   /* resident CTAs per SM the grid is sized for (0 = occupancy maximum) */
+    uint32_t self_check;      /* 1: derive keys at creation and compare with the host derivation */
+} mk_options;
+
+/* One pattern as the reference's GPU needle (Needle, src/service/gpu.rs:618-660):
+ * text needles are base64 characters (lowercase when fold = 1), 1..43 bytes;
+ * regex needles are a DFA table of `len` states × 65 little-endian u16
+ * (src/model/pattern/dfa.rs:189-200: state 0 accepts, state 1 starts, column 64
+ * flags acceptance at the end of input). */
+typedef struct mk_needle {
+    const uint8_t* bytes;
+    uint32_t len;
+    uint32_t fold;
+    uint32_t mode;
+} mk_needle;
+
+/* A candidate hit: its index and the needle it may match.  The GPU tests the
+ * character that depends on the x sign with both values, so a hit is a
+ * candidate that the host confirms (src/service/gpu.rs:973-996). */
+typedef struct mk_hit {
+    uint64_t index;
+    uint32_t needle;
+    uint32_t reserved;
+} mk_hit;
+
+typedef struct mk_info {
+    int device;
+    uint32_t sms;
+    uint32_t grid;            /* CTAs per launch */
+    uint32_t block;           /* threads per CTA */
+    uint32_t keys_per_thread;
+    uint32_t table_rows;
+    uint64_t table_bytes;
+    uint64_t keys_per_iter;   /* grid · block · keys_per_thread */
+    char name[96];
+} mk_info;
+
+typedef struct mk_ctx mk_ctx;
+typedef struct mk_job mk_job;
+
+/* Library ABI version (MK_ABI_VERSION). */
+MK_API uint32_t mk_abi_version(void);
+
+/* Number of CUDA devices (src/service/gpu.rs:1229-1236 device_count); 0 without a driver. */
+MK_API int mk_device_count(void);
+
+/* Gpu::new / Kernel::load (src/service/gpu.rs:678-706, 1162-1216): builds the comb table
+ * on the device and, with self_check, compares derived keys with the host derivation.
+ * On failure *out may still hold a context: read its error with mk_last_error, then
+ * release it with mk_ctx_destroy. */
+MK_API int mk_ctx_create(int device, const mk_options* options, mk_ctx** out);
+MK_API void mk_ctx_destroy(mk_ctx* ctx);
+/* text of the context's last error ("" when none); copies at most size-1 bytes */
+MK_API int mk_last_error(const mk_ctx* ctx, char* buf, size_t size);
+MK_API int mk_ctx_info(const mk_ctx* ctx, mk_info* out);
+/* Engine::keys_per_iter (src/service/gpu.rs:832-834) */
+MK_API uint64_t mk_keys_per_iter(const mk_ctx* ctx);
+
+/* Engine::prepare (src/service/gpu.rs:836-857).  Multiple needles are matched in one
+ * pass; hits carry the needle's position in `needles`. */
+MK_API int mk_job_prepare(mk_ctx* ctx, const uint8_t key[32], int seed_source, const mk_needle* needles,
+                   uint32_t n_needles, int stop_on_hit, mk_job** out);
+MK_API void mk_job_destroy(mk_job* job);
+
+/* Engine::launch (src/service/gpu.rs:859-887): searches indices base .. base +
+ * keys_per_iter·iters - 1, waits, and reports whether any candidate hit was found
+ * (*found = 1, *index = the lowest hit index).  Hits are kept for mk_job_hits. */
+MK_API int mk_job_launch(mk_job* job, uint64_t base, uint32_t iters, int* found, uint64_t* index);
+/* All candidate hits of the last launch in increasing index order (*n = total found,
+ * which may exceed cap; MK_ERR_HIT_RING_FULL when the device ring overflowed). */
+MK_API int mk_job_hits(mk_job* job, mk_hit* out, uint32_t cap, uint32_t* n);
+
+/* Asynchronous form for timing: enqueue one launch on the context's stream without
+ * waiting; mk_ctx_sync waits for all queued work. */
+MK_API int mk_job_enqueue(mk_job* job, uint64_t base, uint32_t iters);
+MK_API int mk_ctx_sync(mk_ctx* ctx);
+/* CUDA events on the context's stream: record into slot (0..15); elapsed ms between two slots */
+MK_API int mk_ctx_record(mk_ctx* ctx, int slot);
+MK_API int mk_ctx_elapsed(mk_ctx* ctx, int from_slot, int to_slot, float* ms);
+
+/* meikey_derive (src/service/gpu/kernel.cu:2062-2069, src/service/gpu.rs:783-804):
+ * n full public keys (x sign included) of indices first..first+n-1 into host `out` (32·n bytes). */
+MK_API int mk_derive(mk_ctx* ctx, const uint8_t key[32], int seed_source, uint64_t first, uint64_t n, uint8_t* out);
+
+/* Comb table entry (row, column) as 24 words (y+x, y-x, 2dxy; row 0 holds 2xy), for tests. */
+MK_API int mk_table_entry(mk_ctx* ctx, uint32_t row, uint64_t col, uint32_t out[24]);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MEIKEY_B200_H */

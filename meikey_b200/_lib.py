@@ -1,0 +1,121 @@
+"""ctypes binding of the in-tree CUDA library (include/meikey_b200.h).
+
+There is no CPU fallback: if ``libmeikey_b200.so`` is missing, loading raises.
+"""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmeikey_b200.so")
+
+# status codes (enum mk_status)
+OK = 0
+ERR_DRIVER_NOT_FOUND = 1
+ERR_NO_DEVICE = 2
+ERR_OUT_OF_RANGE = 3
+ERR_SELF_CHECK = 4
+ERR_NO_SETTINGS = 5
+ERR_CUDA = 6
+ERR_NOT_BUILT = 7
+ERR_BAD_ARG = 8
+ERR_OUT_OF_MEMORY = 9
+ERR_STOPPED = 10
+ERR_HIT_RING_FULL = 11
+ERR_PATTERN = 12
+
+STATUS_NAMES = {
+    OK: "OK", ERR_DRIVER_NOT_FOUND: "DriverNotFound", ERR_NO_DEVICE: "NoDevice",
+    ERR_OUT_OF_RANGE: "OutOfRange", ERR_SELF_CHECK: "SelfCheck", ERR_NO_SETTINGS: "NoSettings",
+    ERR_CUDA: "Driver", ERR_NOT_BUILT: "NotBuilt", ERR_BAD_ARG: "BadArg",
+    ERR_OUT_OF_MEMORY: "OutOfMemory", ERR_STOPPED: "Stopped", ERR_HIT_RING_FULL: "HitRingFull",
+    ERR_PATTERN: "Pattern",
+}
+
+SEED_CHACHA20 = 0
+SEED_COUNTER = 1
+MODE_CONTAINS = 0
+MODE_SUFFIX = 1
+MODE_REGEX = 2
+
+
+class Options(ctypes.Structure):
+    _fields_ = [
+        ("table_rows", ctypes.c_uint32),
+        ("keys_per_thread", ctypes.c_uint32),
+        ("block", ctypes.c_uint32),
+        ("blocks_per_sm", ctypes.c_uint32),
+        ("self_check", ctypes.c_uint32),
+    ]
+
+
+class NeedleC(ctypes.Structure):
+    _fields_ = [
+        ("bytes", ctypes.POINTER(ctypes.c_uint8)),
+        ("len", ctypes.c_uint32),
+        ("fold", ctypes.c_uint32),
+        ("mode", ctypes.c_uint32),
+    ]
+
+
+class HitC(ctypes.Structure):
+    _fields_ = [("index", ctypes.c_uint64), ("needle", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+
+
+class InfoC(ctypes.Structure):
+    _fields_ = [
+        ("device", ctypes.c_int),
+        ("sms", ctypes.c_uint32),
+        ("grid", ctypes.c_uint32),
+        ("block", ctypes.c_uint32),
+        ("keys_per_thread", ctypes.c_uint32),
+        ("table_rows", ctypes.c_uint32),
+        ("table_bytes", ctypes.c_uint64),
+        ("keys_per_iter", ctypes.c_uint64),
+        ("name", ctypes.c_char * 96),
+    ]
+
+
+# (name, restype, argtypes) of every exported function
+SIGNATURES = [
+    ("mk_abi_version", ctypes.c_uint32, []),
+    ("mk_device_count", ctypes.c_int, []),
+    ("mk_ctx_create", ctypes.c_int, [ctypes.c_int, ctypes.POINTER(Options), ctypes.POINTER(ctypes.c_void_p)]),
+    ("mk_ctx_destroy", None, [ctypes.c_void_p]),
+    ("mk_last_error", ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]),
+    ("mk_ctx_info", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(InfoC)]),
+    ("mk_keys_per_iter", ctypes.c_uint64, [ctypes.c_void_p]),
+    ("mk_job_prepare", ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(NeedleC),
+                                      ctypes.c_uint32, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
+    ("mk_job_destroy", None, [ctypes.c_void_p]),
+    ("mk_job_launch", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32, ctypes.POINTER(ctypes.c_int),
+                                     ctypes.POINTER(ctypes.c_uint64)]),
+    ("mk_job_hits", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(HitC), ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32)]),
+    ("mk_job_enqueue", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32]),
+    ("mk_ctx_sync", ctypes.c_int, [ctypes.c_void_p]),
+    ("mk_ctx_record", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    ("mk_ctx_elapsed", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]),
+    ("mk_derive", ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_uint64, ctypes.c_uint64,
+                                 ctypes.c_void_p]),
+    ("mk_table_entry", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64,
+                                      ctypes.POINTER(ctypes.c_uint32)]),
+]
+
+_lib = None
+
+
+def load():
+    """The loaded library; raises OSError when the CUDA build is missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise OSError(
+            f"{LIB_PATH} is missing: build the CUDA library first (python -m meikey_b200.build); "
+            "there is no CPU fallback")
+    lib = ctypes.CDLL(LIB_PATH)
+    for name, res, args in SIGNATURES:
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib

@@ -1,0 +1,474 @@
+// C ABI of the B200 search backend (include/meikey_b200.h).
+//
+// The context owns the device, its stream and the comb table; a job owns the key,
+// the compiled needles and its hit ring.  Every entry point returns a status and
+// records the text of a failure in the context (no exceptions cross the ABI).
+#include <cuda_runtime.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/meikey_b200.h"
+#include "host25519.h"
+#include "kernels.h"
+
+using mkb::CombGeom;
+
+struct mk_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[16] = {};
+    mk_info info{};
+    CombGeom geom{};
+    uint4* table = nullptr;
+    uint32_t kpt = 8, block = 256, grid = 0;
+    std::string err;
+};
+
+struct mk_job {
+    mk_ctx* ctx = nullptr;
+    uint8_t key[32];
+    int source = 0;
+    int stop_on_hit = 0;
+    std::vector<mkh25519::Needle> needles;
+    mkb::MatchSet* d_match = nullptr;
+    std::vector<uint8_t*> d_dfa;
+    mkb::HitRecord* d_hits = nullptr;
+    uint32_t cap = 1u << 16;
+    mkb::JobDevice* d_job = nullptr;
+    uint32_t* d_sink = nullptr;
+    std::vector<mk_hit> last;
+    uint32_t last_total = 0;
+};
+
+namespace {
+
+int fail(mk_ctx* c, int code, const std::string& msg) {
+    if (c) c->err = msg;
+    return code;
+}
+
+int cuda_fail(mk_ctx* c, cudaError_t e, const char* what) {
+    return fail(c, MK_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define MK_CUDA(ctx, call)                                     \
+    do {                                                       \
+        cudaError_t e_ = (call);                               \
+        if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call); \
+    } while (0)
+
+const char B64[] = "ABCDEFGHIJKLMNOPQRSTUVWXYZabcdefghijklmnopqrstuvwxyz0123456789+/";
+
+int b64_value(uint8_t c) {
+    const char* p = c ? strchr(B64, c) : nullptr;
+    return p ? (int)(p - B64) : -1;
+}
+
+// Comb geometry for `rows` rows: rows-1 signed rows of width w or w+1 and a top row
+// of the remaining bits, chosen to minimise the number of entries.
+bool make_geometry(uint32_t rows, CombGeom& g) {
+    if (rows < 3 || rows > (uint32_t)mkb::MAX_ROWS) return false;
+    const uint32_t n = rows - 1;
+    double best = 1e300;
+    uint32_t bw = 0, ba = 0, bt = 0;
+    for (uint32_t w = 2; w <= 27; w++)
+        for (uint32_t a = 0; a < n; a++) {
+            uint32_t used = n * w + a;
+            if (used >= 251) continue;
+            uint32_t t = 251 - used;
+            if (t > 27) continue;
+            double entries = (double)a * ((1u << w) + 1) + (double)(n - a) * ((1u << (w - 1)) + 1) + (double)(1u << t) + 1;
+            if (entries < best) {
+                best = entries;
+                bw = w;
+                ba = a;
+                bt = t;
+            }
+        }
+    if (!bw) return false;
+    memset(&g, 0, sizeof g);
+    g.rows = rows;
+    uint32_t off = 0;
+    uint64_t base = 0;
+    for (uint32_t i = 0; i < rows; i++) {
+        uint32_t w = i + 1 == rows ? bt : (i < ba ? bw + 1 : bw);
+        g.width[i] = w;
+        g.offset[i] = off;
+        g.row_base[i] = base;
+        g.cols[i] = i + 1 == rows ? (1ull << w) + 1 : (1ull << (w - 1)) + 1;
+        off += w;
+        base += g.cols[i];
+    }
+    g.entries = base;
+    return off == 251;
+}
+
+int self_check(mk_ctx* c) {
+    // both seed sources, an odd first index (seed from the second half of a block)
+    const uint64_t n = 257;
+    std::vector<uint8_t> got(32 * n);
+    for (int src = 0; src < 2; src++) {
+        uint8_t key[32];
+        for (int i = 0; i < 32; i++) key[i] = (uint8_t)(0x5a ^ (i * 37 + src * 101));
+        uint64_t first = 0x123456789abull | 1;
+        int st = mk_derive(c, key, src, first, n, got.data());
+        if (st) return st;
+        for (uint64_t i = 0; i < n; i += (i < 8 ? 1 : 31)) {
+            uint8_t seed[32], pk[32];
+            mkh25519::seed_of(key, src, first + i, seed);
+            mkh25519::public_key(seed, pk);
+            if (memcmp(pk, &got[32 * i], 32) != 0)
+                return fail(c, MK_ERR_SELF_CHECK, "GPU public keys differ from the host derivation");
+        }
+    }
+    return MK_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+uint32_t mk_abi_version(void) { return MK_ABI_VERSION; }
+
+int mk_device_count(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) return 0;
+    return n;
+}
+
+int mk_last_error(const mk_ctx* ctx, char* buf, size_t size) {
+    if (!buf || size == 0) return MK_ERR_BAD_ARG;
+    const char* s = ctx ? ctx->err.c_str() : "";
+    snprintf(buf, size, "%s", s);
+    return MK_OK;
+}
+
+int mk_ctx_create(int device, const mk_options* options, mk_ctx** out) {
+    if (!out) return MK_ERR_BAD_ARG;
+    *out = nullptr;
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e == cudaErrorInsufficientDriver || e == cudaErrorNoDevice) return e == cudaErrorNoDevice ? MK_ERR_NO_DEVICE : MK_ERR_DRIVER_NOT_FOUND;
+    if (e != cudaSuccess) return MK_ERR_DRIVER_NOT_FOUND;
+    if (device < 0 || device >= n) return MK_ERR_NO_DEVICE;
+    mk_options o{};
+    if (options) o = *options;
+    if (!o.table_rows) o.table_rows = 12;
+    if (!o.keys_per_thread) o.keys_per_thread = 8;
+    if (!o.block) o.block = 256;
+    if (o.table_rows < 10 || o.table_rows > 16 || (o.keys_per_thread != 4 && o.keys_per_thread != 8 && o.keys_per_thread != 16) ||
+        (o.block != 128 && o.block != 256) || o.blocks_per_sm > 16)
+        return MK_ERR_OUT_OF_RANGE;
+    mk_ctx* c = new (std::nothrow) mk_ctx;
+    if (!c) return MK_ERR_OUT_OF_MEMORY;
+    *out = c;
+    c->device = device;
+    c->kpt = o.keys_per_thread;
+    c->block = o.block;
+    MK_CUDA(c, cudaSetDevice(device));
+    MK_CUDA(c, cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    for (auto& ev : c->ev) MK_CUDA(c, cudaEventCreate(&ev));
+    cudaDeviceProp prop;
+    MK_CUDA(c, cudaGetDeviceProperties(&prop, device));
+    int occ = 0;
+    MK_CUDA(c, mkb::keys_occupancy(false, c->kpt, c->block, &occ));
+    if (occ < 1) return fail(c, MK_ERR_NOT_BUILT, "kernel does not fit on this device");
+    uint32_t per_sm = o.blocks_per_sm ? std::min<uint32_t>(o.blocks_per_sm, (uint32_t)occ) : (uint32_t)occ;
+    c->grid = (uint32_t)prop.multiProcessorCount * per_sm;
+    if (!make_geometry(o.table_rows, c->geom)) return fail(c, MK_ERR_OUT_OF_RANGE, "no comb geometry for this row count");
+    // table
+    size_t bytes = (size_t)c->geom.entries * mkb::ENTRY_WORDS * 4;
+    e = cudaMalloc(&c->table, bytes);
+    if (e != cudaSuccess) {
+        c->table = nullptr;
+        return fail(c, MK_ERR_OUT_OF_MEMORY, "comb table allocation failed");
+    }
+    std::vector<uint32_t> pts = mkh25519::comb_points(c->geom.rows, c->geom.offset);
+    uint32_t* d_pts = nullptr;
+    MK_CUDA(c, cudaMalloc(&d_pts, pts.size() * 4));
+    MK_CUDA(c, cudaMemcpyAsync(d_pts, pts.data(), pts.size() * 4, cudaMemcpyHostToDevice, c->stream));
+    const uint64_t chunk = 1ull << 22;
+    for (uint64_t f = 0; f < c->geom.entries; f += chunk) {
+        uint64_t cnt = std::min<uint64_t>(chunk, c->geom.entries - f);
+        MK_CUDA(c, mkb::launch_build_table(c->table, c->geom, d_pts, f, cnt, c->stream));
+    }
+    MK_CUDA(c, cudaStreamSynchronize(c->stream));
+    cudaFree(d_pts);
+    // info
+    mk_info& in = c->info;
+    in.device = device;
+    in.sms = (uint32_t)prop.multiProcessorCount;
+    in.grid = c->grid;
+    in.block = c->block;
+    in.keys_per_thread = c->kpt;
+    in.table_rows = c->geom.rows;
+    in.table_bytes = bytes;
+    in.keys_per_iter = (uint64_t)c->grid * c->block * c->kpt;
+    snprintf(in.name, sizeof in.name, "%.95s", prop.name);
+    if (o.self_check) {
+        int st = self_check(c);
+        if (st) return st;
+    }
+    return MK_OK;
+}
+
+void mk_ctx_destroy(mk_ctx* c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->table) cudaFree(c->table);
+    for (auto& ev : c->ev)
+        if (ev) cudaEventDestroy(ev);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+int mk_ctx_info(const mk_ctx* c, mk_info* out) {
+    if (!c || !out) return MK_ERR_BAD_ARG;
+    *out = c->info;
+    return MK_OK;
+}
+
+uint64_t mk_keys_per_iter(const mk_ctx* c) { return c ? c->info.keys_per_iter : 0; }
+
+int mk_derive(mk_ctx* c, const uint8_t key[32], int seed_source, uint64_t first, uint64_t n, uint8_t* out) {
+    if (!c || !key || (!out && n) || (seed_source != 0 && seed_source != 1)) return fail(c, MK_ERR_BAD_ARG, "bad argument");
+    if (n == 0) return MK_OK;
+    MK_CUDA(c, cudaSetDevice(c->device));
+    const uint64_t per_launch = 1ull << 22;
+    uint8_t* d_out = nullptr;
+    uint64_t cap = std::min(n, per_launch);
+    MK_CUDA(c, cudaMalloc(&d_out, cap * 32));
+    for (uint64_t done = 0; done < n; done += per_launch) {
+        uint64_t cnt = std::min(per_launch, n - done);
+        mkb::KeyLaunch L{};
+        L.table = c->table;
+        L.geom = c->geom;
+        for (int i = 0; i < 8; i++) L.key[i] = (uint32_t)key[4 * i] | (uint32_t)key[4 * i + 1] << 8 | (uint32_t)key[4 * i + 2] << 16 | (uint32_t)key[4 * i + 3] << 24;
+        L.seed_src = (uint32_t)seed_source;
+        L.iters = 1;
+        L.base = first + done;
+        L.out = d_out;
+        L.count = cnt;
+        uint64_t threads = (cnt + c->kpt - 1) / c->kpt;
+        uint32_t grid = (uint32_t)((threads + c->block - 1) / c->block);
+        cudaError_t e = mkb::launch_keys(L, true, c->kpt, c->block, grid, c->stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(out + 32 * done, d_out, cnt * 32, cudaMemcpyDeviceToHost, c->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) {
+            cudaFree(d_out);
+            return cuda_fail(c, e, "derive");
+        }
+    }
+    cudaFree(d_out);
+    return MK_OK;
+}
+
+int mk_table_entry(mk_ctx* c, uint32_t row, uint64_t col, uint32_t out[24]) {
+    if (!c || !out || row >= c->geom.rows || col >= c->geom.cols[row]) return fail(c, MK_ERR_BAD_ARG, "bad table entry");
+    MK_CUDA(c, cudaSetDevice(c->device));
+    MK_CUDA(c, cudaMemcpy(out, c->table + (c->geom.row_base[row] + col) * (mkb::ENTRY_WORDS / 4), 96, cudaMemcpyDeviceToHost));
+    return MK_OK;
+}
+
+int mk_job_prepare(mk_ctx* c, const uint8_t key[32], int seed_source, const mk_needle* needles, uint32_t n_needles,
+                   int stop_on_hit, mk_job** out) {
+    if (!c || !key || !out || (n_needles && !needles) || (seed_source != 0 && seed_source != 1))
+        return fail(c, MK_ERR_BAD_ARG, "bad argument");
+    if (n_needles > (uint32_t)mkb::MAX_NEEDLES) return fail(c, MK_ERR_BAD_ARG, "too many needles");
+    *out = nullptr;
+    MK_CUDA(c, cudaSetDevice(c->device));
+    mkb::MatchSet* ms = new (std::nothrow) mkb::MatchSet;
+    if (!ms) return fail(c, MK_ERR_OUT_OF_MEMORY, "host allocation");
+    memset(ms, 0, sizeof *ms);
+    mk_job* j = new (std::nothrow) mk_job;
+    if (!j) {
+        delete ms;
+        return fail(c, MK_ERR_OUT_OF_MEMORY, "host allocation");
+    }
+    j->ctx = c;
+    memcpy(j->key, key, 32);
+    j->source = seed_source;
+    j->stop_on_hit = stop_on_hit;
+    auto bail = [&](int code, const std::string& msg) {
+        delete ms;
+        mk_job_destroy(j);
+        return fail(c, code, msg);
+    };
+    uint32_t bit = 0;  // next free bit in the shift-and state
+    for (uint32_t i = 0; i < n_needles; i++) {
+        const mk_needle& nd = needles[i];
+        mkh25519::Needle h;
+        h.mode = nd.mode;
+        h.fold = nd.fold != 0;
+        h.len = nd.len;
+        if (nd.mode == MK_MODE_REGEX) {
+            if (nd.len == 0 || nd.len > 65535 || !nd.bytes) return bail(MK_ERR_BAD_ARG, "bad DFA table");
+            size_t bytes = (size_t)nd.len * 65 * 2;
+            h.bytes.assign(nd.bytes, nd.bytes + bytes);
+            // every transition must name a state of the table
+            for (size_t s = 0; s < nd.len; s++)
+                for (int v = 0; v < 64; v++) {
+                    uint32_t t = h.bytes[(s * 65 + v) * 2] | (uint32_t)h.bytes[(s * 65 + v) * 2 + 1] << 8;
+                    if (t >= nd.len) return bail(MK_ERR_BAD_ARG, "DFA transition out of range");
+                }
+            if (ms->n_regex >= 16) return bail(MK_ERR_BAD_ARG, "at most 16 regex needles per job");
+            uint8_t* d = nullptr;
+            if (cudaMalloc(&d, bytes) != cudaSuccess) return bail(MK_ERR_OUT_OF_MEMORY, "DFA allocation");
+            j->d_dfa.push_back(d);
+            if (cudaMemcpy(d, h.bytes.data(), bytes, cudaMemcpyHostToDevice) != cudaSuccess)
+                return bail(MK_ERR_CUDA, "DFA copy");
+            ms->dfa[ms->n_regex] = d;
+            ms->dfa_states[ms->n_regex] = nd.len;
+            ms->regex_id[ms->n_regex] = (uint16_t)i;
+            ms->n_regex++;
+        } else if (nd.mode == MK_MODE_CONTAINS || nd.mode == MK_MODE_SUFFIX) {
+            if (nd.len == 0 || nd.len > 43 || !nd.bytes) return bail(MK_ERR_BAD_ARG, "needle length must be 1..43");
+            h.bytes.assign(nd.bytes, nd.bytes + nd.len);
+            for (auto& ch : h.bytes) {
+                if (b64_value(ch) < 0) return bail(MK_ERR_PATTERN, "needle character outside the base64 alphabet");
+                if (h.fold && ch >= 'A' && ch <= 'Z') ch = (uint8_t)(ch + 32);
+            }
+            // do not straddle a 64-bit word
+            if ((bit & 63) + nd.len > 64) bit = (bit + 63) & ~63u;
+            if (bit + nd.len > 64u * mkb::SA_WORDS) return bail(MK_ERR_BAD_ARG, "needles exceed the shift-and state");
+            for (uint32_t k = 0; k < nd.len; k++) {
+                uint32_t b = bit + k;
+                uint8_t ch = h.bytes[k];
+                int v = b64_value(ch);
+                ms->mask[v][b >> 6] |= 1ull << (b & 63);
+                if (h.fold && ch >= 'a' && ch <= 'z') ms->mask[v - 26][b >> 6] |= 1ull << (b & 63);
+            }
+            ms->first_bit[bit >> 6] |= 1ull << (bit & 63);
+            uint32_t last = bit + nd.len - 1;
+            if (nd.mode == MK_MODE_SUFFIX) ms->suffix_bit[last >> 6] |= 1ull << (last & 63);
+            else ms->last_bit[last >> 6] |= 1ull << (last & 63);
+            ms->text_id[ms->n_text] = (uint16_t)i;
+            ms->text_last[ms->n_text] = (uint16_t)last;
+            ms->n_text++;
+            bit += nd.len;
+        } else {
+            return bail(MK_ERR_BAD_ARG, "unknown needle mode");
+        }
+        j->needles.push_back(std::move(h));
+    }
+    ms->sa_words = ms->n_text ? (bit + 63) / 64 : 0;
+    if (cudaMalloc(&j->d_match, sizeof *ms) != cudaSuccess) return bail(MK_ERR_OUT_OF_MEMORY, "match allocation");
+    if (cudaMemcpy(j->d_match, ms, sizeof *ms, cudaMemcpyHostToDevice) != cudaSuccess) return bail(MK_ERR_CUDA, "match copy");
+    delete ms;
+    ms = nullptr;
+    auto bail2 = [&](int code, const std::string& msg) {
+        mk_job_destroy(j);
+        return fail(c, code, msg);
+    };
+    if (cudaMalloc(&j->d_hits, sizeof(mkb::HitRecord) * j->cap) != cudaSuccess) return bail2(MK_ERR_OUT_OF_MEMORY, "hit ring");
+    if (cudaMalloc(&j->d_job, sizeof(mkb::JobDevice)) != cudaSuccess) return bail2(MK_ERR_OUT_OF_MEMORY, "job state");
+    if (cudaMemset(j->d_job, 0, sizeof(mkb::JobDevice)) != cudaSuccess) return bail2(MK_ERR_CUDA, "job state");
+    if (cudaMalloc(&j->d_sink, sizeof(uint32_t) * (size_t)c->grid * c->block) != cudaSuccess)
+        return bail2(MK_ERR_OUT_OF_MEMORY, "sink");
+    *out = j;
+    return MK_OK;
+}
+
+void mk_job_destroy(mk_job* j) {
+    if (!j) return;
+    if (j->ctx) cudaSetDevice(j->ctx->device);
+    if (j->ctx && j->ctx->stream) cudaStreamSynchronize(j->ctx->stream);
+    for (auto d : j->d_dfa) cudaFree(d);
+    if (j->d_match) cudaFree(j->d_match);
+    if (j->d_hits) cudaFree(j->d_hits);
+    if (j->d_job) cudaFree(j->d_job);
+    if (j->d_sink) cudaFree(j->d_sink);
+    delete j;
+}
+
+static int enqueue(mk_job* j, uint64_t base, uint32_t iters) {
+    mk_ctx* c = j->ctx;
+    MK_CUDA(c, cudaSetDevice(c->device));
+    MK_CUDA(c, cudaMemsetAsync(j->d_job, 0, 8, c->stream));  // hit_count and status; keep stop
+    mkb::KeyLaunch L{};
+    L.table = c->table;
+    L.geom = c->geom;
+    for (int i = 0; i < 8; i++)
+        L.key[i] = (uint32_t)j->key[4 * i] | (uint32_t)j->key[4 * i + 1] << 8 | (uint32_t)j->key[4 * i + 2] << 16 | (uint32_t)j->key[4 * i + 3] << 24;
+    L.seed_src = (uint32_t)j->source;
+    L.iters = iters;
+    L.base = base;
+    L.match = j->d_match;
+    L.hits = j->d_hits;
+    L.hit_cap = j->cap;
+    L.stop_on_hit = (uint32_t)j->stop_on_hit;
+    L.job = j->d_job;
+    L.sink = j->d_sink;
+    MK_CUDA(c, mkb::launch_keys(L, false, c->kpt, c->block, c->grid, c->stream));
+    return MK_OK;
+}
+
+int mk_job_enqueue(mk_job* j, uint64_t base, uint32_t iters) {
+    if (!j) return MK_ERR_BAD_ARG;
+    if (iters == 0) return MK_OK;
+    return enqueue(j, base, iters);
+}
+
+int mk_job_launch(mk_job* j, uint64_t base, uint32_t iters, int* found, uint64_t* index) {
+    if (!j) return MK_ERR_BAD_ARG;
+    mk_ctx* c = j->ctx;
+    j->last.clear();
+    j->last_total = 0;
+    if (found) *found = 0;
+    if (iters == 0) return MK_OK;
+    int st = enqueue(j, base, iters);
+    if (st) return st;
+    mkb::JobDevice jd;
+    MK_CUDA(c, cudaMemcpyAsync(&jd, j->d_job, sizeof jd, cudaMemcpyDeviceToHost, c->stream));
+    MK_CUDA(c, cudaStreamSynchronize(c->stream));
+    j->last_total = jd.hit_count;
+    uint32_t n = std::min(jd.hit_count, j->cap);
+    if (n) {
+        std::vector<mkb::HitRecord> h(n);
+        MK_CUDA(c, cudaMemcpy(h.data(), j->d_hits, sizeof(mkb::HitRecord) * n, cudaMemcpyDeviceToHost));
+        j->last.resize(n);
+        for (uint32_t i = 0; i < n; i++) j->last[i] = mk_hit{h[i].index, h[i].needle, 0};
+        std::sort(j->last.begin(), j->last.end(),
+                  [](const mk_hit& a, const mk_hit& b) { return a.index != b.index ? a.index < b.index : a.needle < b.needle; });
+        if (found) *found = 1;
+        if (index) *index = j->last[0].index;
+    }
+    if (jd.hit_count > j->cap) return fail(c, MK_ERR_HIT_RING_FULL, "hit ring overflow");
+    if (jd.status & 1u) return MK_ERR_STOPPED;
+    return MK_OK;
+}
+
+int mk_job_hits(mk_job* j, mk_hit* out, uint32_t cap, uint32_t* n) {
+    if (!j || !n || (cap && !out)) return MK_ERR_BAD_ARG;
+    *n = j->last_total;
+    uint32_t k = std::min<uint32_t>(cap, (uint32_t)j->last.size());
+    for (uint32_t i = 0; i < k; i++) out[i] = j->last[i];
+    return j->last_total > j->cap ? MK_ERR_HIT_RING_FULL : MK_OK;
+}
+
+int mk_ctx_sync(mk_ctx* c) {
+    if (!c) return MK_ERR_BAD_ARG;
+    MK_CUDA(c, cudaStreamSynchronize(c->stream));
+    return MK_OK;
+}
+
+int mk_ctx_record(mk_ctx* c, int slot) {
+    if (!c || slot < 0 || slot >= 16) return MK_ERR_BAD_ARG;
+    MK_CUDA(c, cudaEventRecord(c->ev[slot], c->stream));
+    return MK_OK;
+}
+
+int mk_ctx_elapsed(mk_ctx* c, int a, int b, float* ms) {
+    if (!c || !ms || a < 0 || a >= 16 || b < 0 || b >= 16) return MK_ERR_BAD_ARG;
+    MK_CUDA(c, cudaEventSynchronize(c->ev[b]));
+    MK_CUDA(c, cudaEventElapsedTime(ms, c->ev[a], c->ev[b]));
+    return MK_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,225 @@
+// GF(2^255 - 19) in eight 32-bit limbs (radix 2^32), values kept below 2^256
+// (congruent mod p, not canonical).  Products use hand-written mad.lo.cc /
+// madc.hi.cc carry chains; 2^256 is folded back as 38.  Exact integer math, no FP.
+#pragma once
+#include <stdint.h>
+
+namespace mk32 {
+
+typedef uint32_t u32;
+typedef uint64_t u64;
+
+struct fe {
+    u32 v[8];
+};
+
+__device__ __forceinline__ fe fe_zero() {
+    fe r;
+#pragma unroll
+    for (int i = 0; i < 8; i++) r.v[i] = 0;
+    return r;
+}
+
+__device__ __forceinline__ fe fe_small(u32 x) {
+    fe r = fe_zero();
+    r.v[0] = x;
+    return r;
+}
+
+// r = a + b mod 2^256 folded: a carry out of bit 256 adds 38
+__device__ __forceinline__ fe fe_add(const fe& a, const fe& b) {
+    fe r;
+    u32 c;
+    asm("add.cc.u32 %0, %9, %17;\n\t"
+        "addc.cc.u32 %1, %10, %18;\n\t"
+        "addc.cc.u32 %2, %11, %19;\n\t"
+        "addc.cc.u32 %3, %12, %20;\n\t"
+        "addc.cc.u32 %4, %13, %21;\n\t"
+        "addc.cc.u32 %5, %14, %22;\n\t"
+        "addc.cc.u32 %6, %15, %23;\n\t"
+        "addc.cc.u32 %7, %16, %24;\n\t"
+        "addc.u32 %8, 0, 0;\n\t"
+        : "=r"(r.v[0]), "=r"(r.v[1]), "=r"(r.v[2]), "=r"(r.v[3]), "=r"(r.v[4]), "=r"(r.v[5]), "=r"(r.v[6]),
+          "=r"(r.v[7]), "=r"(c)
+        : "r"(a.v[0]), "r"(a.v[1]), "r"(a.v[2]), "r"(a.v[3]), "r"(a.v[4]), "r"(a.v[5]), "r"(a.v[6]), "r"(a.v[7]),
+          "r"(b.v[0]), "r"(b.v[1]), "r"(b.v[2]), "r"(b.v[3]), "r"(b.v[4]), "r"(b.v[5]), "r"(b.v[6]), "r"(b.v[7]));
+    // fold: r += 38·c; a second carry is impossible to miss: it leaves r < 38, and 38 more fits
+    u32 add = 38u * c, c2;
+    asm("add.cc.u32 %0, %0, %9;\n\t"
+        "addc.cc.u32 %1, %1, 0;\n\t"
+        "addc.cc.u32 %2, %2, 0;\n\t"
+        "addc.cc.u32 %3, %3, 0;\n\t"
+        "addc.cc.u32 %4, %4, 0;\n\t"
+        "addc.cc.u32 %5, %5, 0;\n\t"
+        "addc.cc.u32 %6, %6, 0;\n\t"
+        "addc.cc.u32 %7, %7, 0;\n\t"
+        "addc.u32 %8, 0, 0;\n\t"
+        : "+r"(r.v[0]), "+r"(r.v[1]), "+r"(r.v[2]), "+r"(r.v[3]), "+r"(r.v[4]), "+r"(r.v[5]), "+r"(r.v[6]),
+          "+r"(r.v[7]), "=r"(c2)
+        : "r"(add));
+    r.v[0] += 38u * c2;
+    return r;
+}
+
+// r = a - b; a borrow subtracts 38 (2^256 ≡ 38)
+__device__ __forceinline__ fe fe_sub(const fe& a, const fe& b) {
+    fe r;
+    u32 bw;
+    asm("sub.cc.u32 %0, %9, %17;\n\t"
+        "subc.cc.u32 %1, %10, %18;\n\t"
+        "subc.cc.u32 %2, %11, %19;\n\t"
+        "subc.cc.u32 %3, %12, %20;\n\t"
+        "subc.cc.u32 %4, %13, %21;\n\t"
+        "subc.cc.u32 %5, %14, %22;\n\t"
+        "subc.cc.u32 %6, %15, %23;\n\t"
+        "subc.cc.u32 %7, %16, %24;\n\t"
+        "subc.u32 %8, 0, 0;\n\t"
+        : "=r"(r.v[0]), "=r"(r.v[1]), "=r"(r.v[2]), "=r"(r.v[3]), "=r"(r.v[4]), "=r"(r.v[5]), "=r"(r.v[6]),
+          "=r"(r.v[7]), "=r"(bw)
+        : "r"(a.v[0]), "r"(a.v[1]), "r"(a.v[2]), "r"(a.v[3]), "r"(a.v[4]), "r"(a.v[5]), "r"(a.v[6]), "r"(a.v[7]),
+          "r"(b.v[0]), "r"(b.v[1]), "r"(b.v[2]), "r"(b.v[3]), "r"(b.v[4]), "r"(b.v[5]), "r"(b.v[6]), "r"(b.v[7]));
+    // bw is 0 or 0xffffffff
+    u32 sub = 38u & bw, b2;
+    asm("sub.cc.u32 %0, %0, %9;\n\t"
+        "subc.cc.u32 %1, %1, 0;\n\t"
+        "subc.cc.u32 %2, %2, 0;\n\t"
+        "subc.cc.u32 %3, %3, 0;\n\t"
+        "subc.cc.u32 %4, %4, 0;\n\t"
+        "subc.cc.u32 %5, %5, 0;\n\t"
+        "subc.cc.u32 %6, %6, 0;\n\t"
+        "subc.cc.u32 %7, %7, 0;\n\t"
+        "subc.u32 %8, 0, 0;\n\t"
+        : "+r"(r.v[0]), "+r"(r.v[1]), "+r"(r.v[2]), "+r"(r.v[3]), "+r"(r.v[4]), "+r"(r.v[5]), "+r"(r.v[6]),
+          "+r"(r.v[7]), "=r"(b2)
+        : "r"(sub));
+    // a second borrow leaves r >= 2^256 - 38, so 38 less cannot borrow again
+    r.v[0] -= 38u & b2;
+    return r;
+}
+
+// Fold a 512-bit product t[0..15] to 8 words: t_lo + 38·t_hi, then the top word again.
+__device__ __forceinline__ fe fe_reduce512(const u32 t[16]) {
+    fe r;
+    u32 top;
+    // lo parts of 38·t[8+j] into words j, carries through
+    asm("mad.lo.cc.u32 %0, %9, 38, %17;\n\t"
+        "madc.lo.cc.u32 %1, %10, 38, %18;\n\t"
+        "madc.lo.cc.u32 %2, %11, 38, %19;\n\t"
+        "madc.lo.cc.u32 %3, %12, 38, %20;\n\t"
+        "madc.lo.cc.u32 %4, %13, 38, %21;\n\t"
+        "madc.lo.cc.u32 %5, %14, 38, %22;\n\t"
+        "madc.lo.cc.u32 %6, %15, 38, %23;\n\t"
+        "madc.lo.cc.u32 %7, %16, 38, %24;\n\t"
+        "addc.u32 %8, 0, 0;\n\t"
+        : "=r"(r.v[0]), "=r"(r.v[1]), "=r"(r.v[2]), "=r"(r.v[3]), "=r"(r.v[4]), "=r"(r.v[5]), "=r"(r.v[6]),
+          "=r"(r.v[7]), "=r"(top)
+        : "r"(t[8]), "r"(t[9]), "r"(t[10]), "r"(t[11]), "r"(t[12]), "r"(t[13]), "r"(t[14]), "r"(t[15]),
+          "r"(t[0]), "r"(t[1]), "r"(t[2]), "r"(t[3]), "r"(t[4]), "r"(t[5]), "r"(t[6]), "r"(t[7]));
+    // hi parts of 38·t[8+j] into words j+1
+    asm("mad.hi.cc.u32 %1, %9, 38, %1;\n\t"
+        "madc.hi.cc.u32 %2, %10, 38, %2;\n\t"
+        "madc.hi.cc.u32 %3, %11, 38, %3;\n\t"
+        "madc.hi.cc.u32 %4, %12, 38, %4;\n\t"
+        "madc.hi.cc.u32 %5, %13, 38, %5;\n\t"
+        "madc.hi.cc.u32 %6, %14, 38, %6;\n\t"
+        "madc.hi.cc.u32 %7, %15, 38, %7;\n\t"
+        "madc.hi.u32 %8, %16, 38, %8;\n\t"
+        : "+r"(r.v[0]), "+r"(r.v[1]), "+r"(r.v[2]), "+r"(r.v[3]), "+r"(r.v[4]), "+r"(r.v[5]), "+r"(r.v[6]),
+          "+r"(r.v[7]), "+r"(top)
+        : "r"(t[8]), "r"(t[9]), "r"(t[10]), "r"(t[11]), "r"(t[12]), "r"(t[13]), "r"(t[14]), "r"(t[15]));
+    // top < 40: fold 38·top; one more carry is possible and is folded as 38 without further carry
+    u32 add = 38u * top, c2;
+    asm("add.cc.u32 %0, %0, %9;\n\t"
+        "addc.cc.u32 %1, %1, 0;\n\t"
+        "addc.cc.u32 %2, %2, 0;\n\t"
+        "addc.cc.u32 %3, %3, 0;\n\t"
+        "addc.cc.u32 %4, %4, 0;\n\t"
+        "addc.cc.u32 %5, %5, 0;\n\t"
+        "addc.cc.u32 %6, %6, 0;\n\t"
+        "addc.cc.u32 %7, %7, 0;\n\t"
+        "addc.u32 %8, 0, 0;\n\t"
+        : "+r"(r.v[0]), "+r"(r.v[1]), "+r"(r.v[2]), "+r"(r.v[3]), "+r"(r.v[4]), "+r"(r.v[5]), "+r"(r.v[6]),
+          "+r"(r.v[7]), "=r"(c2)
+        : "r"(add));
+    r.v[0] += 38u * c2;
+    return r;
+}
+
+// One row of the operand-scanning product: t[i..i+8] += a · b_i.
+// Even-indexed a_j go in one carry chain (their lo/hi pairs tile words i..i+7),
+// odd-indexed a_j in a second chain (words i+1..i+8).
+#define MK32_ROW(I)                                                                                  \
+    asm("mad.lo.cc.u32 %0, %9, %13, %0;\n\t"                                                        \
+        "madc.hi.cc.u32 %1, %9, %13, %1;\n\t"                                                       \
+        "madc.lo.cc.u32 %2, %10, %13, %2;\n\t"                                                      \
+        "madc.hi.cc.u32 %3, %10, %13, %3;\n\t"                                                      \
+        "madc.lo.cc.u32 %4, %11, %13, %4;\n\t"                                                      \
+        "madc.hi.cc.u32 %5, %11, %13, %5;\n\t"                                                      \
+        "madc.lo.cc.u32 %6, %12, %13, %6;\n\t"                                                      \
+        "madc.hi.cc.u32 %7, %12, %13, %7;\n\t"                                                      \
+        "addc.u32 %8, %8, 0;\n\t"                                                                   \
+        : "+r"(t[I]), "+r"(t[I + 1]), "+r"(t[I + 2]), "+r"(t[I + 3]), "+r"(t[I + 4]), "+r"(t[I + 5]), \
+          "+r"(t[I + 6]), "+r"(t[I + 7]), "+r"(t[I + 8])                                            \
+        : "r"(a.v[0]), "r"(a.v[2]), "r"(a.v[4]), "r"(a.v[6]), "r"(b.v[I]));                         \
+    asm("mad.lo.cc.u32 %0, %8, %12, %0;\n\t"                                                        \
+        "madc.hi.cc.u32 %1, %8, %12, %1;\n\t"                                                       \
+        "madc.lo.cc.u32 %2, %9, %12, %2;\n\t"                                                       \
+        "madc.hi.cc.u32 %3, %9, %12, %3;\n\t"                                                       \
+        "madc.lo.cc.u32 %4, %10, %12, %4;\n\t"                                                      \
+        "madc.hi.cc.u32 %5, %10, %12, %5;\n\t"                                                      \
+        "madc.lo.cc.u32 %6, %11, %12, %6;\n\t"                                                      \
+        "madc.hi.u32 %7, %11, %12, %7;\n\t"                                                         \
+        : "+r"(t[I + 1]), "+r"(t[I + 2]), "+r"(t[I + 3]), "+r"(t[I + 4]), "+r"(t[I + 5]),             \
+          "+r"(t[I + 6]), "+r"(t[I + 7]), "+r"(t[I + 8])                                            \
+        : "r"(a.v[1]), "r"(a.v[3]), "r"(a.v[5]), "r"(a.v[7]), "r"(b.v[I]));
+
+// r = a·b mod p (as a value below 2^256)
+__device__ __forceinline__ fe fe_mul(const fe& a, const fe& b) {
+    u32 t[16];
+#pragma unroll
+    for (int i = 0; i < 16; i++) t[i] = 0;
+    // after row I the partial sum is below 2^(32(I+9)), so word I+8 absorbs the final carry
+    MK32_ROW(0) MK32_ROW(1) MK32_ROW(2) MK32_ROW(3) MK32_ROW(4) MK32_ROW(5) MK32_ROW(6) MK32_ROW(7)
+    return fe_reduce512(t);
+}
+
+__device__ __forceinline__ fe fe_sq(const fe& a) { return fe_mul(a, a); }
+
+// Canonical value (mod p) as 8 words
+__device__ __forceinline__ void fe_to_words(const fe& a, u32 out[8]) {
+    // fold bit 255: x = lo255 + 19·bit255  (< 2^255 + 19)
+    u32 w[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) w[i] = a.v[i];
+    u32 hb = w[7] >> 31;
+    w[7] &= 0x7fffffffu;
+    u64 c = 19ull * hb;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        c += w[i];
+        w[i] = (u32)c;
+        c >>= 32;
+    }
+    // subtract p if x >= p: compute x + 19 and test bit 255
+    u32 t[8];
+    c = 19;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        c += w[i];
+        t[i] = (u32)c;
+        c >>= 32;
+    }
+    u32 ge = t[7] >> 31;
+    t[7] &= 0x7fffffffu;
+#pragma unroll
+    for (int i = 0; i < 8; i++) out[i] = ge ? t[i] : w[i];
+}
+
+__device__ __forceinline__ fe fe_from_words(const u32 w[8]) {
+    fe r;
+#pragma unroll
+    for (int i = 0; i < 8; i++) r.v[i] = w[i];
+    return r;
+}
+
+}  // namespace mk32

@@ -1,0 +1,67 @@
+// Structures shared by the host runtime and the device kernels.
+#pragma once
+#include <stdint.h>
+
+namespace mkb {
+
+// Comb geometry for the fixed-base multiply.
+//
+// A clamped scalar is s = 2^254 + 8·m with m = bits 3..253 (251 bits), so
+// s·B = 2^254·B + Σ_i d_i · (2^(off_i) · 8B) where d_i are the digits of m.
+// Rows 0..rows-2 use signed digits in [-2^(w-1), 2^(w-1)) with a carry into the next
+// row; the top row's digit is unsigned in [0, 2^w_top] and its entries include the
+// 2^254·B term.  Row i holds entries k·2^(off_i)·8B for k = 0..cols_i-1.
+constexpr int MAX_ROWS = 20;
+
+struct CombGeom {
+    uint32_t rows;
+    uint32_t width[MAX_ROWS];
+    uint32_t offset[MAX_ROWS];   // bit offset of digit i inside m
+    uint64_t row_base[MAX_ROWS]; // first entry of row i
+    uint64_t cols[MAX_ROWS];
+    uint64_t entries;
+};
+
+// Words per table entry: (y+x, y-x, 2dxy) canonical, 8 little-endian u32 each.
+constexpr int ENTRY_WORDS = 24;
+
+// Matcher: up to MAX_NEEDLES needles tested in one pass.
+//   text needles (contains / suffix, fold): bit-parallel shift-and over the 43 searched
+//   base64 characters; needle n occupies bits [bit0, bit0+len) of a multi-word state.
+//   regex needles: DFA walk over a states×65×u16 table in device memory.
+constexpr int MAX_NEEDLES = 128;
+constexpr int SA_WORDS = 8;  // shift-and state words (512 bits of concatenated needles)
+
+struct MatchSet {
+    uint32_t n_text;              // text needles packed into the shift-and state
+    uint32_t n_regex;             // regex needles
+    uint32_t sa_words;            // words of shift-and state in use
+    uint32_t pad;
+    // shift-and: per value v (0..63) the bits of needle positions accepting v
+    uint64_t mask[64][SA_WORDS];
+    uint64_t first_bit[SA_WORDS]; // bit 0 of every text needle (set on each step)
+    uint64_t last_bit[SA_WORDS];  // last bit of every contains-needle
+    uint64_t suffix_bit[SA_WORDS];// last bit of every suffix-needle (tested at the end only)
+    uint16_t text_id[MAX_NEEDLES];// caller's needle index per text needle
+    uint16_t text_last[MAX_NEEDLES]; // global bit index of each text needle's last bit
+    // regex needles
+    const uint8_t* dfa[16];
+    uint32_t dfa_states[16];
+    uint16_t regex_id[16];
+};
+
+struct HitRecord {
+    uint64_t index;
+    uint32_t needle;
+    uint32_t reserved;
+};
+
+// Device-side job state for one launch.
+struct JobDevice {
+    uint32_t hit_count;     // total hits found (may exceed capacity)
+    uint32_t status;        // 0 ok, bit 0: stopped on the stop word
+    uint32_t stop;          // host-writable stop word (nonzero stops at the next iteration)
+    uint32_t pad;
+};
+
+}  // namespace mkb
