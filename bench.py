@@ -1,0 +1,372 @@
+"""Benchmark of the candidate-key search path (one JSON line on rank 0).
+
+Workload (the reference's throughput configuration, synthetic inputs): secure-path seeds
+from ChaCha20 with key SHA-256(u64 7 little-endian), a case-sensitive 7-character contains
+needle drawn uniformly from the base64 alphabet with numpy.random.default_rng(7), 2^34
+candidates in total.  A step is one launch over >= 2^30 consecutive candidate indices;
+the default 16 steps cover 2^34.  Multi-GPU: one process per GPU (torchrun), each rank
+searches its own index range (rank·2^56 ...), so the work is weakly scaled with no
+data-path collective; timing is the max over ranks.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+import argparse
+import hashlib
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "keys/s on 1 B200 (bit-exact pubkeys), % int-MAD peak; multi-job p50/p99"
+UNIT = "keys/s"
+ALPHABET = "ABCDEFGHIJKLMNOPQRSTUVWXYZabcdefghijklmnopqrstuvwxyz0123456789+/"
+TOTAL_CANDIDATES = 1 << 34
+STEP_CANDIDATES = 1 << 30
+
+
+def workload_key() -> bytes:
+    return hashlib.sha256((7).to_bytes(8, "little")).digest()
+
+
+def workload_needle() -> str:
+    import numpy as np
+    rng = np.random.default_rng(7)
+    return "".join(ALPHABET[int(i)] for i in rng.integers(0, 64, 7))
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() in ("active", "1"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+class Dist:
+    """Barrier and max-over-ranks for the torchrun case (NCCL); no-ops for one process."""
+
+    def __init__(self, world, local):
+        self.world = world
+        self.pg = None
+        if world > 1:
+            import datetime
+            import torch
+            import torch.distributed as dist
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+            self.torch, self.dist = torch, dist
+            self.pg = True
+
+    def barrier(self):
+        if self.pg:
+            self.dist.barrier()
+
+    def max(self, x: float) -> float:
+        if not self.pg:
+            return x
+        t = self.torch.tensor([x], dtype=self.torch.float64, device="cuda")
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the reference's kernel compiled for the CPU (oracle/_ref) or the oracle port
+# ---------------------------------------------------------------------------
+
+class CpuBaseline:
+    def __init__(self):
+        from oracle import pyoracle
+        self.po = pyoracle
+        self.threads = os.cpu_count() or 1
+        variants = [p for p in pyoracle.ref_variants() if "f8_b32" in p] or pyoracle.ref_variants()
+        if variants:
+            self.kind = "reference"
+            self.ref = pyoracle.RefKernel(variants[0])
+            self.width = 16
+            self.table = pyoracle.ref_table(self.width)
+            self.what = (f"reference kernel.cu compiled as C++ ({os.path.basename(variants[0])}, comb width 16), "
+                         f"its CPU search emulation on {self.threads} threads")
+        else:
+            self.kind = "port"
+            self.ref = None
+            self.what = f"C oracle restatement of the path on {self.threads} threads"
+
+    def run(self, key: bytes, needle: str, seconds: float, base: int = 0):
+        """keys/s over a sample of about `seconds` of work on all threads."""
+        from concurrent.futures import ThreadPoolExecutor
+        nb = needle.encode()
+        if self.ref is not None:
+            per_call = 128 * self.ref.batch  # one block of the emulated kernel per iteration
+
+            def job(t, iters):
+                self.ref.search(128, self.table, self.width, key, False, nb, len(nb), False, 0,
+                                base + t * (1 << 40), iters, False)
+            # calibrate
+            t0 = time.perf_counter()
+            job(0, 1)
+            one = max(time.perf_counter() - t0, 1e-4)
+            iters = max(1, int(seconds / one))
+            t0 = time.perf_counter()
+            with ThreadPoolExecutor(self.threads) as ex:
+                list(ex.map(lambda t: job(t, iters), range(self.threads)))
+            dt = time.perf_counter() - t0
+            keys = self.threads * per_call * iters
+        else:
+            def job(t, n):
+                self.po.search(key, 0, base + t * (1 << 40), n, nb, len(nb), False, 0, threads=1)
+            t0 = time.perf_counter()
+            job(0, 2000)
+            per_key = max((time.perf_counter() - t0) / 2000, 1e-7)
+            n = max(1000, int(seconds / per_key))
+            t0 = time.perf_counter()
+            with ThreadPoolExecutor(self.threads) as ex:
+                list(ex.map(lambda t: job(t, n), range(self.threads)))
+            dt = time.perf_counter() - t0
+            keys = self.threads * n
+        return keys / dt, keys
+
+
+# ---------------------------------------------------------------------------
+# arms
+# ---------------------------------------------------------------------------
+
+def run_reference(args):
+    world, rank, local = dist_env()
+    if rank != 0:
+        return 0
+    key, needle = workload_key(), workload_needle()
+    cpu = CpuBaseline()
+    per_step = args.ref_step_seconds
+    for _ in range(args.warmup):
+        cpu.run(key, needle, per_step / 4)
+    rates, keys = [], 0
+    t0 = time.perf_counter()
+    for s in range(args.steps):
+        r, k = cpu.run(key, needle, per_step, base=(s + 1) << 44)
+        rates.append(r)
+        keys += k
+    dt = time.perf_counter() - t0
+    value = keys / dt
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * dt / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": workload_config(None),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cpu.threads, "kind": cpu.kind,
+                         "sample": f"{keys} candidates over {args.steps} steps; {cpu.what}"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def workload_config(ctx, step_candidates=None, steps=None):
+    cfg = {
+        "workload": "secure-path throughput: ChaCha20 seeds (key SHA-256(u64 7)), SHA-512, clamp, "
+                    "comb multiply, pooled inversion, base64, case-sensitive 7-char contains "
+                    f"'{workload_needle()}' (numpy default_rng(7)); 2^34 candidates",
+        "candidates_total": TOTAL_CANDIDATES,
+    }
+    if ctx is not None:
+        info = ctx.info
+        cfg.update({
+            "step_candidates": step_candidates,
+            "steps_cover": step_candidates * steps if steps else None,
+            "table_rows": info["table_rows"],
+            "table_bytes": info["table_bytes"],
+            "keys_per_thread": info["keys_per_thread"],
+            "block": info["block"],
+            "grid": info["grid"],
+            "inversion_batch": info["keys_per_thread"] * info["block"] // 32,
+            "l2": "inputs larger than L2: random gathers from the comb table in HBM",
+            "parallelism": "one process per GPU, disjoint index ranges (rank * 2^56), no collective",
+        })
+    return cfg
+
+
+def traffic_per_key():
+    path = os.path.join(ROOT, "profiles", "k_search_dram.json")
+    try:
+        with open(path) as f:
+            return json.load(f).get("dram_bytes_per_key")
+    except (OSError, ValueError):
+        return None
+
+
+def run_ours(args):
+    world, rank, local = dist_env()
+    dist = Dist(world, local)
+    import meikey_b200 as mk
+    key, needle = workload_key(), workload_needle()
+    ctx = mk.Context(device=local, table_rows=args.rows, keys_per_thread=args.kpt, block=args.block,
+                     self_check=True)
+    kpi = ctx.keys_per_iter
+    iters = math.ceil(args.step_candidates / kpi)
+    step_keys = kpi * iters
+    rank_base = rank << 56
+    peak = ctx.measure_imad_peak()
+    field_muls, mads_per_key = ctx.work_per_key()
+    job = ctx.job(key, mk.SEED_CHACHA20, [mk.Needle.contains(needle)])
+    # warm-up
+    for w in range(args.warmup):
+        job.enqueue(rank_base + w * step_keys, iters)
+    ctx.sync()
+    # timed region: device-resident inputs, K launches back to back
+    clocks = ClockSampler(local)
+    clocks.start()
+    dist.barrier()
+    ctx.sync()
+    ctx.record(0)
+    first = rank_base + args.warmup * step_keys
+    for s in range(args.steps):
+        job.enqueue(first + s * step_keys, iters)
+    ctx.record(1)
+    ctx.sync()
+    dist.barrier()
+    ms_local = ctx.elapsed_ms(0, 1)
+    clk = clocks.stop()
+    ms = dist.max(ms_local)
+    keys_all = step_keys * args.steps * world
+    value = keys_all / (ms / 1000.0)
+    per_gpu = step_keys * args.steps / (ms_local / 1000.0)
+    # end to end through the public API: prepare (H2D of key + compiled needle), launch,
+    # read the job state and hits back (D2H), confirm hits on the host
+    e2e_steps = args.e2e_steps or args.steps
+    h2d = d2h = 0
+    found = 0
+    dist.barrier()
+    t0 = time.perf_counter()
+    for s in range(e2e_steps):
+        with ctx.job(key, mk.SEED_CHACHA20, [mk.Needle.contains(needle)]) as j:
+            j.launch(first + (args.steps + s) * step_keys, iters)
+            hits, total = j.hits()
+            found += total
+            a, b = j.io_bytes()
+            h2d += a
+            d2h += b
+    dt_e2e = time.perf_counter() - t0
+    dt_e2e = dist.max(dt_e2e)
+    e2e = step_keys * e2e_steps * world / dt_e2e
+    job.close()
+    ctx_info = dict(ctx.info)
+    line = None
+    if rank == 0:
+        achieved = mads_per_key * per_gpu / 1e12
+        tpk = traffic_per_key()
+        roofline = {
+            "bound": "int_mad", "achieved": achieved, "peak": peak / 1e12, "unit": "Tmad/s",
+            "frac": achieved / (peak / 1e12) if peak else None,
+            "traffic": tpk * step_keys if tpk else None,
+            "peak_source": "measured live: mad.lo.u32 independent chains at full occupancy (mk_measure_imad_peak)",
+            "work_per_key": {"field_muls": field_muls, "int_mads": mads_per_key},
+            "kernel_ms_per_launch": ms_local / args.steps,
+        }
+        cfg = workload_config(ctx, step_keys, args.steps)
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32", "data": "synthetic", "config": cfg, "clocks": clk,
+            "gpu_launches": args.steps,
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d // e2e_steps,
+                    "d2h_bytes_per_step": d2h // e2e_steps, "steps": e2e_steps, "hits_found": found},
+            "roofline": roofline,
+            "device": ctx_info["name"],
+        }
+    ctx.close()
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = CpuBaseline()
+        rate, keys = cpu.run(key, needle, args.cpu_seconds)
+        line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cpu.threads, "kind": cpu.kind,
+                                "sample": f"{keys} candidates of the same workload; {cpu.what}"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    dist.close()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=16)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--rows", type=int, default=12, help="comb table rows")
+    ap.add_argument("--kpt", type=int, default=16, help="keys per thread")
+    ap.add_argument("--block", type=int, default=512)
+    ap.add_argument("--e2e-steps", type=int, default=0, help="end-to-end steps (default: --steps)")
+    ap.add_argument("--step-candidates", type=int, default=STEP_CANDIDATES,
+                    help="candidates per step (default 2^30; smaller only for profiling captures)")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample length")
+    ap.add_argument("--ref-step-seconds", type=float, default=2.0, help="reference arm: seconds per step")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

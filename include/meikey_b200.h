@@ -62,10 +62,12 @@ enum mk_mode { MK_MODE_CONTAINS = 0, MK_MODE_SUFFIX = 1, MK_MODE_REGEX = 2 };
  * means fewer point additions per key and a larger table in HBM). */
 typedef struct mk_options {
     uint32_t table_rows;      /* 10..16; default 12 */
-    uint32_t keys_per_thread; /* keys one thread derives before the pooled inversion: 4, 8 or 16 */
-    uint32_t block;           /* threads per CTA: 128 or 256 */
+    uint32_t keys_per_thread; /* keys one thread derives before the pooled inversion (default 16) */
+    uint32_t block;           /* threads per CTA (default 512): 256 (keys per thread 4, 8, 16) or 512 (8, 16);
+                                 the last warp of a search CTA only inverts */
     uint32_t blocks_per_sm;   /* resident CTAs per SM the grid is sized for (0 = occupancy maximum) */
     uint32_t self_check;      /* 1: derive keys at creation and compare with the host derivation */
+    uint32_t hit_capacity;    /* hit-ring entries per job (0 = 65536) */
 } mk_options;
 
 /* One pattern as the reference's GPU needle (Needle, src/service/gpu.rs:618-660):
@@ -97,7 +99,7 @@ typedef struct mk_info {
     uint32_t keys_per_thread;
     uint32_t table_rows;
     uint64_t table_bytes;
-    uint64_t keys_per_iter;   /* grid · block · keys_per_thread */
+    uint64_t keys_per_iter;   /* grid · (block - 32) · keys_per_thread */
     char name[96];
 } mk_info;
 
@@ -132,9 +134,10 @@ MK_API void mk_job_destroy(mk_job* job);
  * keys_per_iter·iters - 1, waits, and reports whether any candidate hit was found
  * (*found = 1, *index = the lowest hit index).  Hits are kept for mk_job_hits. */
 MK_API int mk_job_launch(mk_job* job, uint64_t base, uint32_t iters, int* found, uint64_t* index);
-/* All candidate hits of the last launch in increasing index order (*n = total found,
- * which may exceed cap; MK_ERR_HIT_RING_FULL when the device ring overflowed). */
-MK_API int mk_job_hits(mk_job* job, mk_hit* out, uint32_t cap, uint32_t* n);
+/* Candidate hits of the last launch in increasing index order: writes min(cap, kept)
+ * records and sets *written to that number; *total is every hit found, which exceeds the
+ * number kept when the device ring overflowed (then MK_ERR_HIT_RING_FULL is returned). */
+MK_API int mk_job_hits(mk_job* job, mk_hit* out, uint32_t cap, uint32_t* written, uint64_t* total);
 
 /* Asynchronous form for timing: enqueue one launch on the context's stream without
  * waiting; mk_ctx_sync waits for all queued work. */
@@ -150,6 +153,19 @@ MK_API int mk_derive(mk_ctx* ctx, const uint8_t key[32], int seed_source, uint64
 
 /* Comb table entry (row, column) as 24 words (y+x, y-x, 2dxy; row 0 holds 2xy), for tests. */
 MK_API int mk_table_entry(mk_ctx* ctx, uint32_t row, uint64_t col, uint32_t out[24]);
+
+/* Bytes the job has copied host->device and device->host so far (kernel parameters,
+ * compiled needles, job state and hit records), for end-to-end accounting. */
+MK_API int mk_job_io_bytes(const mk_job* job, uint64_t* h2d, uint64_t* d2h);
+
+/* Field multiplications and 32-bit integer multiply-adds per key of the configured
+ * search kernel (the algorithmic count: comb additions, batch-inversion share, compression). */
+MK_API int mk_ctx_work_per_key(const mk_ctx* ctx, double* field_muls, double* int_mads);
+
+/* Measured peak of 32-bit integer multiply-adds (mad.lo.u32, independent chains, full
+ * occupancy, best of three bounded runs of about 20 ms) on the context's device, in MADs/s.
+ * This is the denominator of the int-MAD roofline (the reference reports none). */
+MK_API int mk_measure_imad_peak(mk_ctx* ctx, double* mads_per_s);
 
 #ifdef __cplusplus
 }

@@ -45,6 +45,7 @@ class Options(ctypes.Structure):
         ("block", ctypes.c_uint32),
         ("blocks_per_sm", ctypes.c_uint32),
         ("self_check", ctypes.c_uint32),
+        ("hit_capacity", ctypes.c_uint32),
     ]
 
 
@@ -89,7 +90,8 @@ SIGNATURES = [
     ("mk_job_destroy", None, [ctypes.c_void_p]),
     ("mk_job_launch", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32, ctypes.POINTER(ctypes.c_int),
                                      ctypes.POINTER(ctypes.c_uint64)]),
-    ("mk_job_hits", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(HitC), ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32)]),
+    ("mk_job_hits", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(HitC), ctypes.c_uint32,
+                                   ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint64)]),
     ("mk_job_enqueue", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32]),
     ("mk_ctx_sync", ctypes.c_int, [ctypes.c_void_p]),
     ("mk_ctx_record", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
@@ -98,6 +100,11 @@ SIGNATURES = [
                                  ctypes.c_void_p]),
     ("mk_table_entry", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint64,
                                       ctypes.POINTER(ctypes.c_uint32)]),
+    ("mk_job_io_bytes", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64),
+                                       ctypes.POINTER(ctypes.c_uint64)]),
+    ("mk_ctx_work_per_key", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
+                                           ctypes.POINTER(ctypes.c_double)]),
+    ("mk_measure_imad_peak", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]),
 ]
 
 _lib = None

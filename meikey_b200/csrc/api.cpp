@@ -26,6 +26,7 @@ struct mk_ctx {
     CombGeom geom{};
     uint4* table = nullptr;
     uint32_t kpt = 8, block = 256, grid = 0;
+    uint32_t hit_capacity = 1u << 16;
     std::string err;
 };
 
@@ -43,6 +44,7 @@ struct mk_job {
     uint32_t* d_sink = nullptr;
     std::vector<mk_hit> last;
     uint32_t last_total = 0;
+    uint64_t h2d = 0, d2h = 0;  // bytes copied for this job
 };
 
 namespace {
@@ -159,10 +161,11 @@ int mk_ctx_create(int device, const mk_options* options, mk_ctx** out) {
     mk_options o{};
     if (options) o = *options;
     if (!o.table_rows) o.table_rows = 12;
-    if (!o.keys_per_thread) o.keys_per_thread = 8;
-    if (!o.block) o.block = 256;
-    if (o.table_rows < 10 || o.table_rows > 16 || (o.keys_per_thread != 4 && o.keys_per_thread != 8 && o.keys_per_thread != 16) ||
-        (o.block != 128 && o.block != 256) || o.blocks_per_sm > 16)
+    if (!o.keys_per_thread) o.keys_per_thread = 16;
+    if (!o.block) o.block = 512;
+    const bool built = (o.block == 256 && (o.keys_per_thread == 4 || o.keys_per_thread == 8 || o.keys_per_thread == 16)) ||
+                       (o.block == 512 && (o.keys_per_thread == 8 || o.keys_per_thread == 16));
+    if (o.table_rows < 10 || o.table_rows > 16 || !built || o.blocks_per_sm > 16 || o.hit_capacity > (1u << 26))
         return MK_ERR_OUT_OF_RANGE;
     mk_ctx* c = new (std::nothrow) mk_ctx;
     if (!c) return MK_ERR_OUT_OF_MEMORY;
@@ -170,6 +173,7 @@ int mk_ctx_create(int device, const mk_options* options, mk_ctx** out) {
     c->device = device;
     c->kpt = o.keys_per_thread;
     c->block = o.block;
+    if (o.hit_capacity) c->hit_capacity = o.hit_capacity;
     MK_CUDA(c, cudaSetDevice(device));
     MK_CUDA(c, cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     for (auto& ev : c->ev) MK_CUDA(c, cudaEventCreate(&ev));
@@ -208,7 +212,8 @@ int mk_ctx_create(int device, const mk_options* options, mk_ctx** out) {
     in.keys_per_thread = c->kpt;
     in.table_rows = c->geom.rows;
     in.table_bytes = bytes;
-    in.keys_per_iter = (uint64_t)c->grid * c->block * c->kpt;
+    // the search kernel's last warp per CTA inverts; the others derive keys
+    in.keys_per_iter = (uint64_t)c->grid * (c->block - 32) * c->kpt;
     snprintf(in.name, sizeof in.name, "%.95s", prop.name);
     if (o.self_check) {
         int st = self_check(c);
@@ -295,6 +300,7 @@ int mk_job_prepare(mk_ctx* c, const uint8_t key[32], int seed_source, const mk_n
     memcpy(j->key, key, 32);
     j->source = seed_source;
     j->stop_on_hit = stop_on_hit;
+    j->cap = c->hit_capacity;
     auto bail = [&](int code, const std::string& msg) {
         delete ms;
         mk_job_destroy(j);
@@ -323,6 +329,7 @@ int mk_job_prepare(mk_ctx* c, const uint8_t key[32], int seed_source, const mk_n
             j->d_dfa.push_back(d);
             if (cudaMemcpy(d, h.bytes.data(), bytes, cudaMemcpyHostToDevice) != cudaSuccess)
                 return bail(MK_ERR_CUDA, "DFA copy");
+            j->h2d += bytes;
             ms->dfa[ms->n_regex] = d;
             ms->dfa_states[ms->n_regex] = nd.len;
             ms->regex_id[ms->n_regex] = (uint16_t)i;
@@ -360,6 +367,7 @@ int mk_job_prepare(mk_ctx* c, const uint8_t key[32], int seed_source, const mk_n
     ms->sa_words = ms->n_text ? (bit + 63) / 64 : 0;
     if (cudaMalloc(&j->d_match, sizeof *ms) != cudaSuccess) return bail(MK_ERR_OUT_OF_MEMORY, "match allocation");
     if (cudaMemcpy(j->d_match, ms, sizeof *ms, cudaMemcpyHostToDevice) != cudaSuccess) return bail(MK_ERR_CUDA, "match copy");
+    j->h2d += sizeof *ms;
     delete ms;
     ms = nullptr;
     auto bail2 = [&](int code, const std::string& msg) {
@@ -406,6 +414,7 @@ static int enqueue(mk_job* j, uint64_t base, uint32_t iters) {
     L.job = j->d_job;
     L.sink = j->d_sink;
     MK_CUDA(c, mkb::launch_keys(L, false, c->kpt, c->block, c->grid, c->stream));
+    j->h2d += sizeof L;  // kernel parameters
     return MK_OK;
 }
 
@@ -427,11 +436,13 @@ int mk_job_launch(mk_job* j, uint64_t base, uint32_t iters, int* found, uint64_t
     mkb::JobDevice jd;
     MK_CUDA(c, cudaMemcpyAsync(&jd, j->d_job, sizeof jd, cudaMemcpyDeviceToHost, c->stream));
     MK_CUDA(c, cudaStreamSynchronize(c->stream));
+    j->d2h += sizeof jd;
     j->last_total = jd.hit_count;
     uint32_t n = std::min(jd.hit_count, j->cap);
     if (n) {
         std::vector<mkb::HitRecord> h(n);
         MK_CUDA(c, cudaMemcpy(h.data(), j->d_hits, sizeof(mkb::HitRecord) * n, cudaMemcpyDeviceToHost));
+        j->d2h += sizeof(mkb::HitRecord) * n;
         j->last.resize(n);
         for (uint32_t i = 0; i < n; i++) j->last[i] = mk_hit{h[i].index, h[i].needle, 0};
         std::sort(j->last.begin(), j->last.end(),
@@ -444,12 +455,48 @@ int mk_job_launch(mk_job* j, uint64_t base, uint32_t iters, int* found, uint64_t
     return MK_OK;
 }
 
-int mk_job_hits(mk_job* j, mk_hit* out, uint32_t cap, uint32_t* n) {
-    if (!j || !n || (cap && !out)) return MK_ERR_BAD_ARG;
-    *n = j->last_total;
+int mk_job_hits(mk_job* j, mk_hit* out, uint32_t cap, uint32_t* written, uint64_t* total) {
+    if (!j || !written || !total || (cap && !out)) return MK_ERR_BAD_ARG;
+    *total = j->last_total;
     uint32_t k = std::min<uint32_t>(cap, (uint32_t)j->last.size());
     for (uint32_t i = 0; i < k; i++) out[i] = j->last[i];
+    *written = k;
     return j->last_total > j->cap ? MK_ERR_HIT_RING_FULL : MK_OK;
+}
+
+int mk_job_io_bytes(const mk_job* j, uint64_t* h2d, uint64_t* d2h) {
+    if (!j || !h2d || !d2h) return MK_ERR_BAD_ARG;
+    *h2d = j->h2d;
+    *d2h = j->d2h;
+    return MK_OK;
+}
+
+int mk_ctx_work_per_key(const mk_ctx* c, double* field_muls, double* int_mads) {
+    if (!c || !field_muls || !int_mads) return MK_ERR_BAD_ARG;
+    // radix-2^32 costs: a multiplication is 64 mad.lo + 64 mad.hi (8x8 limbs) + 16 (fold by 38),
+    // a squaring 28 cross products + 8 diagonal ones (72) + 16
+    const double MUL = 144.0, SQ = 88.0;
+    const double kpt = c->kpt, rows = c->geom.rows;
+    const double ct = c->block - 32.0, groups = ct / 32.0;
+    // comb: row 0 is free, full additions cost 7 multiplications, the last one 3
+    double comb = 7.0 * (rows - 2) + 3.0;
+    // Montgomery batch inside a thread: a_j and the running product (2 each for j > 0),
+    // back-sweep y_j = a_j·inv and inv·den_j
+    double batch = (4.0 * (kpt - 1) + 1.0) / kpt;
+    // pooled inversion by the CTA's inverter warp: each lane a pool of `groups` thread
+    // products, 3(groups-1) multiplications and one inversion (254 squarings + 11 multiplications)
+    double pool_mul = 32.0 * (3.0 * (groups - 1) + 11.0) / (ct * kpt);
+    double pool_sq = 32.0 * 254.0 / (ct * kpt);
+    *field_muls = comb + batch + pool_mul + pool_sq;
+    *int_mads = (comb + batch + pool_mul) * MUL + pool_sq * SQ;
+    return MK_OK;
+}
+
+int mk_measure_imad_peak(mk_ctx* c, double* mads_per_s) {
+    if (!c || !mads_per_s) return MK_ERR_BAD_ARG;
+    MK_CUDA(c, cudaSetDevice(c->device));
+    MK_CUDA(c, mkb::measure_imad((int)c->info.sms, c->stream, mads_per_s));
+    return MK_OK;
 }
 
 int mk_ctx_sync(mk_ctx* c) {

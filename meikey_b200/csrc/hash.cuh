@@ -23,7 +23,7 @@ typedef uint64_t u64;
 __device__ __forceinline__ void chacha20_block(const u32 key[8], u64 counter, u32 out[16]) {
     u32 x[16] = {0x61707865u, 0x3320646eu, 0x79622d32u, 0x6b206574u, key[0], key[1], key[2], key[3],
                  key[4],      key[5],      key[6],      key[7],      (u32)counter, (u32)(counter >> 32), 0u, 0u};
-#pragma unroll
+#pragma unroll 1
     for (int r = 0; r < 10; r++) {
         MKH_QR(x[0], x[4], x[8], x[12]);
         MKH_QR(x[1], x[5], x[9], x[13]);
@@ -91,12 +91,13 @@ __device__ __forceinline__ void sha512_round(u64& a, u64& b, u64& c, u64& d, u64
     h = g; g = f; f = e; e = d + t1; d = c; c = b; b = a; a = t1 + s0 + mj;
 }
 
-// State (a..h) at the start of round `from` and the message words w0..w3 (big-endian
-// seed words); runs rounds from..79 of the single padded block and writes the clamped
-// scalar as 4 little-endian u64 words (s = h0..h3 + IV, bytes big-endian).
-// `w16`/`w17` are the schedule words 16 and 17 when from > 0 (they depend on w0..w2 only).
+// Rounds FROM..79 of the single padded block whose message words 0..3 are `w4`
+// (words 4..15 are the fixed padding of a 32-byte message), from state `st` at the
+// start of round FROM; writes the clamped scalar as 4 little-endian u64 words
+// (s = h0..h3 + IV read little-endian).  Rounds 16..79 run as a rolled loop of
+// 16-round blocks so the code stays small; schedule indices stay static inside a block.
 template <int FROM>
-__device__ __forceinline__ void sha512_scalar_from(u64 st[8], const u64 w4[4], u64 w16, u64 w17, u64 s_out[4]) {
+__device__ __forceinline__ void sha512_scalar_from(const u64 st[8], const u64 w4[4], u64 s_out[4]) {
     u64 w[16];
 #pragma unroll
     for (int i = 0; i < 4; i++) w[i] = w4[i];
@@ -106,25 +107,17 @@ __device__ __forceinline__ void sha512_scalar_from(u64 st[8], const u64 w4[4], u
     w[15] = 256;
     u64 a = st[0], b = st[1], c = st[2], d = st[3], e = st[4], f = st[5], g = st[6], h = st[7];
 #pragma unroll
-    for (int t = 0; t < 80; t++) {
-        if (t < FROM) continue;
-        u64 wt;
-        if (t < 16) {
-            wt = w[t];
-        } else if (FROM > 0 && t == 16) {
-            wt = w16;
-            w[0] = wt;
-        } else if (FROM > 0 && t == 17) {
-            wt = w17;
-            w[1] = wt;
-        } else {
-            u64 x15 = w[(t + 1) & 15], x2 = w[(t + 14) & 15];
+    for (int t = FROM; t < 16; t++) sha512_round(a, b, c, d, e, f, g, h, w[t], SHA512_K[t]);
+#pragma unroll 1
+    for (int blk = 16; blk < 80; blk += 16) {
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+            u64 x15 = w[(i + 1) & 15], x2 = w[(i + 14) & 15];
             u64 s0 = rotr64(x15, 1) ^ rotr64(x15, 8) ^ (x15 >> 7);
             u64 s1 = rotr64(x2, 19) ^ rotr64(x2, 61) ^ (x2 >> 6);
-            wt = w[t & 15] + s0 + w[(t + 9) & 15] + s1;
-            w[t & 15] = wt;
+            w[i] = w[i] + s0 + w[(i + 9) & 15] + s1;
+            sha512_round(a, b, c, d, e, f, g, h, w[i], SHA512_K[blk + i]);
         }
-        sha512_round(a, b, c, d, e, f, g, h, wt, SHA512_K[t]);
     }
     u64 hh[4] = {a + MKH_IV0, b + MKH_IV1, c + MKH_IV2, d + MKH_IV3};
 #pragma unroll
@@ -145,16 +138,15 @@ __device__ __forceinline__ void seed_scalar(const u32 sw[8], u64 s_out[4]) {
 #pragma unroll
     for (int i = 0; i < 4; i++) w4[i] = (u64)bswap32(sw[2 * i]) << 32 | bswap32(sw[2 * i + 1]);
     u64 st[8] = {MKH_IV0, MKH_IV1, MKH_IV2, MKH_IV3, MKH_IV4, MKH_IV5, MKH_IV6, MKH_IV7};
-    sha512_scalar_from<0>(st, w4, 0, 0, s_out);
+    sha512_scalar_from<0>(st, w4, s_out);
 }
 
 // Low-security seeds (src/model/search.rs:45-50): bytes 0..23 of the base are shared,
-// bytes 24..31 hold (LE tail of base) + index.  The first three SHA-512 rounds and
-// schedule words 16, 17 depend only on the shared part.
+// bytes 24..31 hold (LE tail of base) + index, so message words 0..2 and the first
+// three rounds are the same for every index and are computed once per thread.
 struct CounterMid {
     u64 st[8];   // state before round 3
     u64 w[3];    // message words 0..2
-    u64 w16, w17;
     u64 tail;    // LE u64 of base bytes 24..31
 };
 
@@ -167,14 +159,6 @@ __device__ __forceinline__ CounterMid counter_mid(const u32 base[8]) {
 #pragma unroll
     for (int t = 0; t < 3; t++) sha512_round(a, b, c, d, e, f, g, h, m.w[t], SHA512_K[t]);
     m.st[0] = a; m.st[1] = b; m.st[2] = c; m.st[3] = d; m.st[4] = e; m.st[5] = f; m.st[6] = g; m.st[7] = h;
-    // w16 = σ1(w14) + w9 + σ0(w1) + w0 ; w17 = σ1(w15) + w10 + σ0(w2) + w1  (w9 = w10 = w14 = 0, w15 = 256)
-    u64 x = m.w[1];
-    u64 s0_1 = rotr64(x, 1) ^ rotr64(x, 8) ^ (x >> 7);
-    x = m.w[2];
-    u64 s0_2 = rotr64(x, 1) ^ rotr64(x, 8) ^ (x >> 7);
-    u64 s1_15 = rotr64(256ull, 19) ^ rotr64(256ull, 61) ^ (256ull >> 6);
-    m.w16 = s0_1 + m.w[0];
-    m.w17 = s1_15 + s0_2 + m.w[1];
     return m;
 }
 
@@ -182,13 +166,8 @@ __device__ __forceinline__ void counter_scalar(const CounterMid& m, u64 index, u
     u64 tail = m.tail + index;
     // seed bytes 24..31 = LE(tail); message word 3 reads them big-endian
     u64 w3 = (u64)bswap32((u32)tail) << 32 | bswap32((u32)(tail >> 32));
-    u64 st[8];
-#pragma unroll
-    for (int i = 0; i < 8; i++) st[i] = m.st[i];
-    // round 3 with its message word
-    sha512_round(st[0], st[1], st[2], st[3], st[4], st[5], st[6], st[7], w3, SHA512_K[3]);
     u64 w4[4] = {m.w[0], m.w[1], m.w[2], w3};
-    sha512_scalar_from<4>(st, w4, m.w16, m.w17, s_out);
+    sha512_scalar_from<3>(m.st, w4, s_out);
 }
 
 }  // namespace mkh

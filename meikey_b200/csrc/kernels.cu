@@ -106,9 +106,55 @@ __global__ void __launch_bounds__(256) k_build_table(uint4* table, const CombGeo
 // the fused key kernel
 // ---------------------------------------------------------------------------
 
+// Per-thread staging slots for the comb table: entry of row r is fetched with cp.async
+// (16-byte LDGSTS, L2 only) into slot r & 1 one row ahead of its use.
+struct EntrySlot {
+    uint4 q[2][6];
+};
+
+__device__ __forceinline__ void fetch_entry(EntrySlot& slot, int which, const uint4* table, u64 idx) {
+    const uint4* src = table + idx * (ENTRY_WORDS / 4);
+    u32 dst = (u32)__cvta_generic_to_shared(&slot.q[which][0]);
+#pragma unroll
+    for (int q = 0; q < 6; q++)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst + 16 * q), "l"(src + q) : "memory");
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+
+template <int N>
+__device__ __forceinline__ void wait_entries() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+__device__ __forceinline__ niels read_entry(const EntrySlot& slot, int which) {
+    niels n;
+    const uint4* q = slot.q[which];
+    uint4 a;
+    a = q[0]; n.ypx.v[0] = a.x; n.ypx.v[1] = a.y; n.ypx.v[2] = a.z; n.ypx.v[3] = a.w;
+    a = q[1]; n.ypx.v[4] = a.x; n.ypx.v[5] = a.y; n.ypx.v[6] = a.z; n.ypx.v[7] = a.w;
+    a = q[2]; n.ymx.v[0] = a.x; n.ymx.v[1] = a.y; n.ymx.v[2] = a.z; n.ymx.v[3] = a.w;
+    a = q[3]; n.ymx.v[4] = a.x; n.ymx.v[5] = a.y; n.ymx.v[6] = a.z; n.ymx.v[7] = a.w;
+    a = q[4]; n.t2d.v[0] = a.x; n.t2d.v[1] = a.y; n.t2d.v[2] = a.z; n.t2d.v[3] = a.w;
+    a = q[5]; n.t2d.v[4] = a.x; n.t2d.v[5] = a.y; n.t2d.v[6] = a.z; n.t2d.v[7] = a.w;
+    return n;
+}
+
+// signed digit of row `row` (rows before the top one), updating the carry
+__device__ __forceinline__ int next_digit(const CombGeom& g, const u64 m[4], u32 row, int& carry) {
+    u32 w = g.width[row];
+    int v = (int)bits_at(m, g.offset[row], w) + carry;
+    carry = (v + (1 << (w - 1))) >> w;
+    return v - (carry << w);
+}
+
+__device__ __forceinline__ u64 entry_index(const CombGeom& g, u32 row, int d) {
+    return g.row_base[row] + (u64)(d < 0 ? -d : d);
+}
+
 // Comb multiply: s (clamped, 4 LE words) -> y = yn/yd (and x = xn/xd when wanted).
-__device__ __forceinline__ void comb_mul(const uint4* __restrict__ table, const CombGeom& g, const u64 s[4], fe& yn,
-                                         fe& yd, fe* xn, fe* xd) {
+// Row r's entry is fetched while row r-1 is being added.
+__device__ __forceinline__ void comb_mul(const uint4* __restrict__ table, const CombGeom& g, const u64 s[4],
+                                         EntrySlot& slot, fe& yn, fe& yd, fe* xn, fe* xd) {
     // m = bits 3..253 of s
     u64 m[4];
     m[0] = s[0] >> 3 | s[1] << 61;
@@ -117,17 +163,16 @@ __device__ __forceinline__ void comb_mul(const uint4* __restrict__ table, const 
     m[3] = (s[3] >> 3) & ((1ull << (251 - 192)) - 1ull);
     const u32 rows = g.rows;
     int carry = 0;
+    int d0 = next_digit(g, m, 0, carry);
+    fetch_entry(slot, 0, table, entry_index(g, 0, d0));
+    int dn = next_digit(g, m, 1, carry);  // rows >= 3, so row 1 is not the top row
+    fetch_entry(slot, 1, table, entry_index(g, 1, dn));
     // row 0 -> extended coordinates (X = 2x, Y = 2y, Z = 2, T = 2xy)
+    wait_entries<1>();
     ge P;
     {
-        u32 w = g.width[0];
-        int v = (int)bits_at(m, g.offset[0], w) + carry;
-        int half = 1 << (w - 1);
-        carry = (v + half) >> w;
-        int d = v - (carry << w);
-        bool neg = d < 0;
-        u32 ad = neg ? (u32)(-d) : (u32)d;
-        niels n = load_entry(table, g.row_base[0] + ad);
+        niels n = read_entry(slot, 0);
+        const bool neg = d0 < 0;
         mk32::fe_cswap(n.ypx, n.ymx, neg);
         P.X = mk32::fe_sub(n.ypx, n.ymx);
         P.Y = mk32::fe_add(n.ypx, n.ymx);
@@ -138,22 +183,18 @@ __device__ __forceinline__ void comb_mul(const uint4* __restrict__ table, const 
     }
 #pragma unroll 1
     for (u32 row = 1; row + 1 < rows; row++) {
-        u32 w = g.width[row];
-        int v = (int)bits_at(m, g.offset[row], w) + carry;
-        int half = 1 << (w - 1);
-        carry = (v + half) >> w;
-        int d = v - (carry << w);
-        bool neg = d < 0;
-        u32 ad = neg ? (u32)(-d) : (u32)d;
-        niels n = load_entry(table, g.row_base[row] + ad);
-        P = mk32::ge_add_niels(P, n, neg);
+        const int d = dn;
+        // prefetch row+1 (the top row's digit is unsigned: the carry lands in it unchanged)
+        if (row + 2 < rows) dn = next_digit(g, m, row + 1, carry);
+        else dn = (int)bits_at(m, g.offset[row + 1], g.width[row + 1]) + carry;
+        fetch_entry(slot, (row + 1) & 1, table, entry_index(g, row + 1, dn));
+        wait_entries<1>();
+        niels n = read_entry(slot, row & 1);
+        P = mk32::ge_add_niels(P, n, d < 0);
     }
-    {
-        u32 row = rows - 1;
-        int d = (int)bits_at(m, g.offset[row], g.width[row]) + carry;  // in [0, 2^w_top]
-        niels n = load_entry(table, g.row_base[row] + (u32)d);
-        mk32::ge_add_niels_frac(P, n, yn, yd, xn, xd);
-    }
+    wait_entries<0>();
+    niels n = read_entry(slot, (rows - 1) & 1);
+    mk32::ge_add_niels_frac(P, n, yn, yd, xn, xd);
 }
 
 // 6-bit values of the 44-character base64 tail of the key blob (0x20 then the key),
@@ -254,173 +295,298 @@ __device__ __forceinline__ void report_hits(const u64 hw[2], u64 index, HitRecor
     }
 }
 
-template <int KPT, int BLOCK, bool DERIVE>
-__global__ void __launch_bounds__(BLOCK, 512 / BLOCK) k_keys(const KeyLaunch L) {
-    constexpr int NUM = DERIVE ? 2 * KPT : KPT;
-    constexpr int GROUPS = BLOCK / 32;
-    __shared__ fe pool[2][BLOCK];
+// Seed of index `idx` -> clamped scalar.  `blk`/`blk_id` cache the ChaCha20 block
+// shared by an even index and the next odd one.
+__device__ __forceinline__ void scalar_of(u32 seed_src, const u32 key[8], const mkh::CounterMid& mid, u64 idx,
+                                          u32 blk[16], u64& blk_id, u64 s[4]) {
+    if (seed_src == 1) {
+        mkh::counter_scalar(mid, idx, s);
+    } else {
+        if ((idx >> 1) != blk_id) {
+            blk_id = idx >> 1;
+            mkh::chacha20_block(key, blk_id, blk);
+        }
+        u32 sw[8];
+        const bool odd = idx & 1;
+#pragma unroll
+        for (int i = 0; i < 8; i++) sw[i] = odd ? blk[8 + i] : blk[i];
+        mkh::seed_scalar(sw, s);
+    }
+}
+
+// Batch state of one iteration of one thread (Montgomery's trick with two field elements
+// per key): a[j] = num_j · den_0 ··· den_(j-1) and den[j]; `prod` = den_0 ··· den_(KPT-1).
+// With inv = 1/prod the back-sweep gives y_j = a[j] · inv_j, inv_(j-1) = inv_j · den[j].
+template <int KPT>
+struct Batch {
+    fe a[KPT], den[KPT];
+    fe prod;
+};
+
+// Seeds and clamped scalars of KPT consecutive indices (ALU work: ChaCha20, SHA-512).
+template <int KPT>
+__device__ __forceinline__ void scalars(const KeyLaunch& L, const u32 key[8], const mkh::CounterMid& mid, u64 first,
+                                        u64 sc[KPT][4]) {
+    u32 blk[16];
+    u64 blk_id = ~0ull;
+#pragma unroll 1
+    for (int j = 0; j < KPT; j++) scalar_of(L.seed_src, key, mid, first + (u64)j, blk, blk_id, sc[j]);
+}
+
+// Comb multiplies of the KPT scalars (IMAD work) into the batch.
+template <int KPT>
+__device__ __forceinline__ void combs(const KeyLaunch& L, const CombGeom& g, const u64 sc[KPT][4], EntrySlot& slot,
+                                      Batch<KPT>& b) {
+    fe run;
+#pragma unroll 1
+    for (int j = 0; j < KPT; j++) {
+        fe num;
+        comb_mul(L.table, g, sc[j], slot, num, b.den[j], nullptr, nullptr);
+        if (j == 0) {
+            b.a[0] = num;
+            run = b.den[0];
+        } else {
+            b.a[j] = mk32::fe_mul(num, run);
+            run = mk32::fe_mul(run, b.den[j]);
+        }
+    }
+    b.prod = run;
+}
+
+// Backward pass: `inv` is 1/(product of the batch's denominators); yields each key's
+// canonical y (sign bit 0), tests the needles and reports candidate hits.
+template <int KPT>
+__device__ __forceinline__ void backward(const KeyLaunch& L, const MatchSet& ms, u64 first, const Batch<KPT>& b,
+                                         fe inv, u32& sink) {
+#pragma unroll 1
+    for (int j = KPT - 1; j >= 0; j--) {
+        u32 pk[8];
+        mk32::fe_to_words(mk32::fe_mul(b.a[j], inv), pk);
+        if (j > 0) inv = mk32::fe_mul(inv, b.den[j]);
+        sink ^= pk[7];
+        u64 hw[2];
+        match_key(ms, pk, hw);
+        const bool any = (hw[0] | hw[1]) != 0;
+        // warp ballot: the (rare) warps with a hit compact their records into the ring
+        if (__ballot_sync(0xffffffffu, any)) report_hits(hw, first + (u64)j, L.hits, L.hit_cap, L.job);
+    }
+}
+
+// Named barriers of the search pipeline: products of buffer b ready (1 + b), inverses of
+// buffer b ready (3 + b).  Barrier 0 is __syncthreads.
+__device__ __forceinline__ void bar_sync(int id, int count) { asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory"); }
+__device__ __forceinline__ void bar_arrive(int id, int count) { asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(count) : "memory"); }
+
+// Inverts `groups`·32 products in place: lane l of the calling warp handles the strided
+// pool l, l+32, l+64, ... (Montgomery's trick inside each pool).
+__device__ __forceinline__ void invert_pools(fe* prod, fe* scratch, int groups) {
+    const int l = threadIdx.x & 31;
+    fe acc = prod[l];
+    scratch[l] = acc;
+#pragma unroll 1
+    for (int k = 1; k < groups; k++) {
+        acc = mk32::fe_mul(acc, prod[l + 32 * k]);
+        scratch[l + 32 * k] = acc;
+    }
+    fe inv = mk32::fe_invert(acc);
+#pragma unroll 1
+    for (int k = groups - 1; k > 0; k--) {
+        fe t = mk32::fe_mul(inv, scratch[l + 32 * (k - 1)]);
+        inv = mk32::fe_mul(inv, prod[l + 32 * k]);
+        prod[l + 32 * k] = t;
+    }
+    prod[l] = inv;
+}
+
+// Search kernel.  The CTA's last warp only inverts; the other BLOCK-32 threads each handle
+// KPT consecutive indices per iteration (index = base + (it·nthreads + gid)·KPT + j, where
+// gid and nthreads count these compute threads).  Iterations are pipelined two deep: a
+// compute thread runs the forward pass of iteration it+1 before the backward pass of it,
+// and the inverter turns the CTA's products of iteration it into their inverses in between.
+// Named barriers: products of buffer b ready (1 + b): compute warps arrive, the inverter
+// waits; inverses of buffer b ready (3 + b): the inverter arrives, compute warps wait.
+// Stop requests (host stop word, or a hit with stop_on_hit) are read by the inverter and
+// take effect two iterations later, at a point every warp agrees on.
+template <int KPT, int BLOCK>
+__global__ void __launch_bounds__(BLOCK, 512 / BLOCK) k_search(const KeyLaunch L) {
+    constexpr int CT = BLOCK - 32;      // compute threads
+    constexpr int CW = CT / 32;         // compute warps = pool length per inverter lane
+    extern __shared__ uint4 dyn_smem[];
+    fe (*prod)[CT] = reinterpret_cast<fe (*)[CT]>(dyn_smem);
+    fe (*scratch)[CT] = prod + 2;
+    EntrySlot* slots = reinterpret_cast<EntrySlot*>(scratch + 2);
     __shared__ CombGeom g;
     __shared__ MatchSet ms;
     __shared__ u32 key[8];
+    __shared__ mkh::CounterMid mid;
+    __shared__ volatile u32 stop_iter;
     const u32 tid = threadIdx.x;
-    const u64 gid = (u64)blockIdx.x * BLOCK + tid;
-    const u64 nthreads = (u64)gridDim.x * BLOCK;
-    // stage launch constants in shared memory
     {
         const u32* src = (const u32*)&L.geom;
         u32* dst = (u32*)&g;
         for (u32 i = tid; i < sizeof(CombGeom) / 4; i += BLOCK) dst[i] = src[i];
-        if (!DERIVE) {
-            const u32* s2 = (const u32*)L.match;
-            u32* d2 = (u32*)&ms;
-            for (u32 i = tid; i < sizeof(MatchSet) / 4; i += BLOCK) d2[i] = s2[i];
+        const u32* s2 = (const u32*)L.match;
+        u32* d2 = (u32*)&ms;
+        for (u32 i = tid; i < sizeof(MatchSet) / 4; i += BLOCK) d2[i] = s2[i];
+        if (tid < 8) key[tid] = L.key[tid];
+        if (tid == 0) stop_iter = L.iters;
+    }
+    __syncthreads();
+    if (tid == 0 && L.seed_src == 1) mid = mkh::counter_mid(key);
+    __syncthreads();
+    const u32 iters = L.iters;
+    if (iters == 0) return;
+
+    if (tid >= (u32)CT) {
+        // ---- inverter warp ----
+        for (u32 it = 0;; it++) {
+            const int b = it & 1;
+            bar_sync(1 + b, BLOCK);
+            if ((tid & 31) == 0) {
+                const volatile JobDevice* jd = L.job;
+                if (jd->stop != 0 || (L.stop_on_hit && jd->hit_count != 0)) {
+                    u32 s = it + 2;
+                    if (s < stop_iter) stop_iter = s;
+                }
+            }
+            __syncwarp();
+            invert_pools(prod[b], scratch[b], CW);
+            __syncwarp();
+            bar_arrive(3 + b, BLOCK);
+            if (it + 1 >= iters || it + 1 >= stop_iter) break;
         }
+        if ((tid & 31) == 0 && stop_iter < iters) atomicOr(&L.job->status, 1u);
+        return;
+    }
+
+    // ---- compute warps ----
+    const u64 gid = (u64)blockIdx.x * CT + tid;
+    const u64 nthreads = (u64)gridDim.x * CT;
+    EntrySlot& slot = slots[tid];
+    Batch<KPT> batch[2];
+    u64 sc[KPT][4];
+    u32 sink = 0;
+    auto first_of = [&](u32 it) { return L.base + ((u64)it * nthreads + gid) * KPT; };
+    auto produce = [&](u32 it) {
+        const int b = it & 1;
+        scalars<KPT>(L, key, mid, first_of(it), sc);
+        combs<KPT>(L, g, sc, slot, batch[b]);
+        prod[b][tid] = batch[b].prod;
+        bar_arrive(1 + b, BLOCK);
+    };
+    produce(0);
+    for (u32 it = 0;; it++) {
+        const int b = it & 1;
+        if (it + 1 < iters && it + 1 < stop_iter) produce(it + 1);
+        bar_sync(3 + b, BLOCK);
+        backward<KPT>(L, ms, first_of(it), batch[b], prod[b][tid], sink);
+        if (it + 1 >= iters || it + 1 >= stop_iter) break;
+    }
+    if (L.sink) L.sink[gid] = sink;
+}
+
+// Derive kernel: full public keys (x sign included) of indices base .. base+count-1;
+// one iteration, per-CTA pooled inversion of 2·KPT denominators per thread.
+template <int KPT, int BLOCK>
+__global__ void __launch_bounds__(BLOCK, 512 / BLOCK) k_derive(const KeyLaunch L) {
+    constexpr int NUM = 2 * KPT;
+    extern __shared__ uint4 dyn_smem[];
+    fe* prod = reinterpret_cast<fe*>(dyn_smem);
+    fe* scratch = prod + BLOCK;
+    EntrySlot* slots = reinterpret_cast<EntrySlot*>(scratch + BLOCK);
+    __shared__ CombGeom g;
+    __shared__ u32 key[8];
+    const u32 tid = threadIdx.x;
+    const u64 gid = (u64)blockIdx.x * BLOCK + tid;
+    {
+        const u32* src = (const u32*)&L.geom;
+        u32* dst = (u32*)&g;
+        for (u32 i = tid; i < sizeof(CombGeom) / 4; i += BLOCK) dst[i] = src[i];
         if (tid < 8) key[tid] = L.key[tid];
     }
     __syncthreads();
     mkh::CounterMid mid;
     if (L.seed_src == 1) mid = mkh::counter_mid(key);
-
-    const u32 iters = DERIVE ? 1u : L.iters;
-    u32 sink = 0;
-    for (u32 it = 0; it < iters; it++) {
-        if (!DERIVE) {
-            bool stop = false;
-            if (tid == 0) {
-                volatile JobDevice* jd = L.job;
-                stop = jd->stop != 0 || (L.stop_on_hit && jd->hit_count != 0);
-            }
-            if (__syncthreads_or(stop)) {
-                if (tid == 0) atomicOr(&L.job->status, 1u);
-                break;
-            }
-        }
-        const u64 first = L.base + ((u64)it * nthreads + gid) * KPT;
-        fe num[NUM], den[NUM], pre[NUM];
-        u32 blk[16];
-        u64 blk_id = ~0ull;
+    const u64 first = L.base + gid * KPT;
+    fe num[NUM], den[NUM], pre[NUM];
+    u32 blk[16];
+    u64 blk_id = ~0ull;
 #pragma unroll 1
-        for (int j = 0; j < KPT; j++) {
-            const u64 idx = first + (u64)j;
-            u64 s[4];
-            if (L.seed_src == 1) {
-                mkh::counter_scalar(mid, idx, s);
-            } else {
-                if ((idx >> 1) != blk_id) {
-                    blk_id = idx >> 1;
-                    mkh::chacha20_block(key, blk_id, blk);
-                }
-                u32 sw[8];
-                const bool odd = idx & 1;
-#pragma unroll
-                for (int i = 0; i < 8; i++) sw[i] = odd ? blk[8 + i] : blk[i];
-                mkh::seed_scalar(sw, s);
-            }
-            if (DERIVE) {
-                comb_mul(L.table, g, s, num[2 * j], den[2 * j], &num[2 * j + 1], &den[2 * j + 1]);
-                pre[2 * j] = j == 0 ? den[0] : mk32::fe_mul(pre[2 * j - 1], den[2 * j]);
-                pre[2 * j + 1] = mk32::fe_mul(pre[2 * j], den[2 * j + 1]);
-            } else {
-                comb_mul(L.table, g, s, num[j], den[j], nullptr, nullptr);
-                pre[j] = j == 0 ? den[0] : mk32::fe_mul(pre[j - 1], den[j]);
-            }
-        }
-        // pooled inversion: lane L of warp 0 inverts the products of threads L, L+32, ...
-        const int buf = it & 1;
-        pool[buf][tid] = pre[NUM - 1];
-        __syncthreads();
-        if (tid < 32) {
-            fe acc = pool[buf][tid];
-            pool[buf ^ 1][tid] = acc;
+    for (int j = 0; j < KPT; j++) {
+        u64 s[4];
+        scalar_of(L.seed_src, key, mid, first + (u64)j, blk, blk_id, s);
+        comb_mul(L.table, g, s, slots[tid], num[2 * j], den[2 * j], &num[2 * j + 1], &den[2 * j + 1]);
+        pre[2 * j] = j == 0 ? den[0] : mk32::fe_mul(pre[2 * j - 1], den[2 * j]);
+        pre[2 * j + 1] = mk32::fe_mul(pre[2 * j], den[2 * j + 1]);
+    }
+    prod[tid] = pre[NUM - 1];
+    __syncthreads();
+    if (tid < 32) invert_pools(prod, scratch, BLOCK / 32);
+    __syncthreads();
+    fe inv = prod[tid];
 #pragma unroll 1
-            for (int k = 1; k < GROUPS; k++) {
-                acc = mk32::fe_mul(acc, pool[buf][tid + 32 * k]);
-                pool[buf ^ 1][tid + 32 * k] = acc;
-            }
-            fe inv = mk32::fe_invert(acc);
-#pragma unroll 1
-            for (int k = GROUPS - 1; k > 0; k--) {
-                fe t = mk32::fe_mul(inv, pool[buf ^ 1][tid + 32 * (k - 1)]);
-                inv = mk32::fe_mul(inv, pool[buf][tid + 32 * k]);
-                pool[buf][tid + 32 * k] = t;
-            }
-            pool[buf][tid] = inv;
-        }
-        __syncthreads();
-        fe inv = pool[buf][tid];
-        // back-sweep: element e's inverse is inv·pre[e-1]; then inv·den[e] moves to e-1
-#pragma unroll 1
-        for (int j = KPT - 1; j >= 0; j--) {
-            const u64 idx = first + (u64)j;
-            u32 pk[8];
-            if (DERIVE) {
-                const int ex = 2 * j + 1, ey = 2 * j;
-                fe xinv = mk32::fe_mul(inv, pre[ex - 1]);
-                inv = mk32::fe_mul(inv, den[ex]);
-                fe yinv = ey == 0 ? inv : mk32::fe_mul(inv, pre[ey - 1]);
-                if (ey > 0) inv = mk32::fe_mul(inv, den[ey]);
-                u32 xw[8];
-                mk32::fe_to_words(mk32::fe_mul(num[ex], xinv), xw);
-                mk32::fe_to_words(mk32::fe_mul(num[ey], yinv), pk);
-                pk[7] |= (xw[0] & 1u) << 31;
-                if (idx - L.base < L.count) {
-                    uint4* o = (uint4*)(L.out + (idx - L.base) * 32);
-                    o[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
-                    o[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
-                }
-            } else {
-                fe zinv = j == 0 ? inv : mk32::fe_mul(inv, pre[j - 1]);
-                if (j > 0) inv = mk32::fe_mul(inv, den[j]);
-                mk32::fe_to_words(mk32::fe_mul(num[j], zinv), pk);
-                sink ^= pk[7];
-                u64 hw[2];
-                match_key(ms, pk, hw);
-                const bool any = (hw[0] | hw[1]) != 0;
-                // warp ballot: the (rare) warps with a hit compact their records into the ring
-                if (__ballot_sync(0xffffffffu, any)) report_hits(hw, idx, L.hits, L.hit_cap, L.job);
-            }
+    for (int j = KPT - 1; j >= 0; j--) {
+        const u64 idx = first + (u64)j;
+        const int ex = 2 * j + 1, ey = 2 * j;
+        fe xinv = mk32::fe_mul(inv, pre[ex - 1]);
+        inv = mk32::fe_mul(inv, den[ex]);
+        fe yinv = ey == 0 ? inv : mk32::fe_mul(inv, pre[ey - 1]);
+        if (ey > 0) inv = mk32::fe_mul(inv, den[ey]);
+        u32 xw[8], pk[8];
+        mk32::fe_to_words(mk32::fe_mul(num[ex], xinv), xw);
+        mk32::fe_to_words(mk32::fe_mul(num[ey], yinv), pk);
+        pk[7] |= (xw[0] & 1u) << 31;
+        if (idx - L.base < L.count) {
+            uint4* o = (uint4*)(L.out + (idx - L.base) * 32);
+            o[0] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+            o[1] = make_uint4(pk[4], pk[5], pk[6], pk[7]);
         }
     }
-    if (!DERIVE && L.sink) L.sink[gid] = sink;
 }
 
 // ---------------------------------------------------------------------------
 // host launch wrappers
 // ---------------------------------------------------------------------------
 
-template <int KPT, int BLOCK>
-static cudaError_t launch_keys_t(const KeyLaunch& L, bool derive, uint32_t grid, cudaStream_t st) {
-    if (derive) k_keys<KPT, BLOCK, true><<<grid, BLOCK, 0, st>>>(L);
-    else k_keys<KPT, BLOCK, false><<<grid, BLOCK, 0, st>>>(L);
-    return cudaGetLastError();
+#define MK_VARIANTS(X) X(4, 256) X(8, 256) X(16, 256) X(8, 512) X(16, 512)
+
+// dynamic shared memory: products and inversion scratch (two buffers each for the
+// search pipeline) and the per-thread table staging slots
+static size_t dyn_bytes(bool derive, uint32_t block) {
+    const size_t fe_bytes = 32;
+    const size_t threads = derive ? block : block - 32;  // the search kernel's last warp only inverts
+    return (derive ? 2 : 4) * threads * fe_bytes + threads * sizeof(EntrySlot);
+}
+
+static const void* kernel_of(bool derive, uint32_t kpt, uint32_t block) {
+#define MK_FN(K, B) \
+    if (kpt == K && block == B) return derive ? (const void*)k_derive<K, B> : (const void*)k_search<K, B>;
+    MK_VARIANTS(MK_FN)
+#undef MK_FN
+    return nullptr;
+}
+
+static cudaError_t prepare(const void* f, size_t dyn) {
+    return cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
 }
 
 cudaError_t launch_keys(const KeyLaunch& L, bool derive, uint32_t kpt, uint32_t block, uint32_t grid, cudaStream_t st) {
-    if (block == 256) {
-        switch (kpt) {
-            case 4: return launch_keys_t<4, 256>(L, derive, grid, st);
-            case 8: return launch_keys_t<8, 256>(L, derive, grid, st);
-            case 16: return launch_keys_t<16, 256>(L, derive, grid, st);
-        }
-    } else if (block == 128) {
-        switch (kpt) {
-            case 4: return launch_keys_t<4, 128>(L, derive, grid, st);
-            case 8: return launch_keys_t<8, 128>(L, derive, grid, st);
-            case 16: return launch_keys_t<16, 128>(L, derive, grid, st);
-        }
-    }
-    return cudaErrorInvalidValue;
+    const void* f = kernel_of(derive, kpt, block);
+    if (!f) return cudaErrorInvalidValue;
+    const size_t dyn = dyn_bytes(derive, block);
+    cudaError_t e = prepare(f, dyn);
+    if (e != cudaSuccess) return e;
+    void* args[] = {const_cast<KeyLaunch*>(&L)};
+    return cudaLaunchKernel(f, dim3(grid), dim3(block), args, dyn, st);
 }
 
 cudaError_t keys_occupancy(bool derive, uint32_t kpt, uint32_t block, int* blocks_per_sm) {
-    const void* f = nullptr;
-#define MK_OCC(K, B)                                                                       \
-    if (kpt == K && block == B)                                                            \
-        f = derive ? (const void*)k_keys<K, B, true> : (const void*)k_keys<K, B, false>;
-    MK_OCC(4, 256) MK_OCC(8, 256) MK_OCC(16, 256) MK_OCC(4, 128) MK_OCC(8, 128) MK_OCC(16, 128)
-#undef MK_OCC
+    const void* f = kernel_of(derive, kpt, block);
     if (!f) return cudaErrorInvalidValue;
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, f, (int)block, 0);
+    const size_t dyn = dyn_bytes(derive, block);
+    cudaError_t e = prepare(f, dyn);
+    if (e != cudaSuccess) return e;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, f, (int)block, dyn);
 }
 
 cudaError_t launch_build_table(uint4* table, const CombGeom& g, const uint32_t* points, uint64_t first,
@@ -428,6 +594,53 @@ cudaError_t launch_build_table(uint4* table, const CombGeom& g, const uint32_t* 
     uint32_t blocks = (uint32_t)((count + 255) / 256);
     k_build_table<<<blocks, 256, 0, st>>>(table, g, points, first, count);
     return cudaGetLastError();
+}
+
+}  // namespace mkb
+
+namespace mkb {
+
+// Peak of independent 32-bit multiply-adds: 8 chains per thread, no memory traffic.
+__global__ void __launch_bounds__(256) k_imad_peak(uint32_t iters, uint32_t x, uint32_t y, uint32_t* out) {
+    uint32_t a[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) a[i] = threadIdx.x + i;
+    for (uint32_t it = 0; it < iters; it++) {
+#pragma unroll
+        for (int i = 0; i < 8; i++) asm volatile("mad.lo.u32 %0, %0, %1, %2;" : "+r"(a[i]) : "r"(x), "r"(y));
+    }
+    uint32_t s = 0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) s ^= a[i];
+    out[(uint64_t)blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+cudaError_t measure_imad(int sms, cudaStream_t st, double* mads_per_s) {
+    const uint32_t blocks = (uint32_t)sms * 8, threads = 256, iters = 1u << 17;
+    uint32_t* out = nullptr;
+    cudaError_t e = cudaMalloc(&out, sizeof(uint32_t) * blocks * threads);
+    if (e != cudaSuccess) return e;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    double best = 0;
+    k_imad_peak<<<blocks, threads, 0, st>>>(iters / 16, 0x12345u, 0x9876u, out);  // warm-up
+    for (int rep = 0; rep < 3 && e == cudaSuccess; rep++) {
+        cudaEventRecord(e0, st);
+        k_imad_peak<<<blocks, threads, 0, st>>>(iters, 0x12345u + rep, 0x9876u, out);
+        cudaEventRecord(e1, st);
+        e = cudaEventSynchronize(e1);
+        if (e == cudaSuccess) e = cudaGetLastError();
+        float ms = 0;
+        if (e == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+        double ops = (double)blocks * threads * iters * 8;
+        if (ms > 0 && ops / (ms * 1e-3) > best) best = ops / (ms * 1e-3);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(out);
+    *mads_per_s = best;
+    return e;
 }
 
 }  // namespace mkb

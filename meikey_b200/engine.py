@@ -58,10 +58,10 @@ def _check(lib, ctx_ptr, status: int):
 class Context:
     """A device with the comb table built on it (Gpu::new / Kernel::load)."""
 
-    def __init__(self, device: int = 0, table_rows: int = 12, keys_per_thread: int = 8, block: int = 256,
-                 blocks_per_sm: int = 0, self_check: bool = False):
+    def __init__(self, device: int = 0, table_rows: int = 12, keys_per_thread: int = 16, block: int = 512,
+                 blocks_per_sm: int = 0, self_check: bool = False, hit_capacity: int = 0):
         self._lib = L.load()
-        opts = L.Options(table_rows, keys_per_thread, block, blocks_per_sm, 1 if self_check else 0)
+        opts = L.Options(table_rows, keys_per_thread, block, blocks_per_sm, 1 if self_check else 0, hit_capacity)
         ptr = ctypes.c_void_p()
         st = self._lib.mk_ctx_create(device, ctypes.byref(opts), ctypes.byref(ptr))
         self._ptr = ptr
@@ -94,6 +94,18 @@ class Context:
 
     def job(self, key: bytes, source: int, needles: Sequence[Needle], stop_on_hit: bool = False) -> "Job":
         return Job(self, key, source, needles, stop_on_hit)
+
+    def work_per_key(self):
+        """(field multiplications, 32-bit integer MADs) per key of the search kernel."""
+        fm, im = ctypes.c_double(), ctypes.c_double()
+        _check(self._lib, self._ptr, self._lib.mk_ctx_work_per_key(self._ptr, ctypes.byref(fm), ctypes.byref(im)))
+        return fm.value, im.value
+
+    def measure_imad_peak(self) -> float:
+        """Measured 32-bit integer MADs per second of the device (bounded microbenchmark)."""
+        v = ctypes.c_double()
+        _check(self._lib, self._ptr, self._lib.mk_measure_imad_peak(self._ptr, ctypes.byref(v)))
+        return v.value
 
     def sync(self):
         _check(self._lib, self._ptr, self._lib.mk_ctx_sync(self._ptr))
@@ -156,12 +168,17 @@ class Job:
     def hits(self, cap: int = 1 << 16) -> Tuple[List[Tuple[int, int]], int]:
         """Candidate hits (index, needle) of the last launch, sorted, and the total count."""
         out = (L.HitC * cap)()
-        n = ctypes.c_uint32()
-        st = self._lib.mk_job_hits(self._ptr, out, cap, ctypes.byref(n))
+        written, total = ctypes.c_uint32(), ctypes.c_uint64()
+        st = self._lib.mk_job_hits(self._ptr, out, cap, ctypes.byref(written), ctypes.byref(total))
         if st not in (L.OK, L.ERR_HIT_RING_FULL):
             _check(self._lib, self.ctx._ptr, st)
-        k = min(cap, n.value)
-        return [(int(out[i].index), int(out[i].needle)) for i in range(k)], int(n.value)
+        return [(int(out[i].index), int(out[i].needle)) for i in range(written.value)], int(total.value)
+
+    def io_bytes(self):
+        """(host->device, device->host) bytes this job has copied so far."""
+        a, b = ctypes.c_uint64(), ctypes.c_uint64()
+        _check(self._lib, self.ctx._ptr, self._lib.mk_job_io_bytes(self._ptr, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
 
     def enqueue(self, base: int, iters: int):
         _check(self._lib, self.ctx._ptr, self._lib.mk_job_enqueue(self._ptr, base, iters))

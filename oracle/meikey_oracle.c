@@ -389,6 +389,15 @@ EXPORT void mko_base_mul(const u8 s[32], u8 pk[32]) {
     ge_compress(base_mul(s), pk);
 }
 
+/* affine coordinates (canonical LE bytes) of s·B for a 256-bit little-endian scalar */
+EXPORT void mko_point_affine(const u8 s[32], u8 x_out[32], u8 y_out[32]) {
+    oracle_init();
+    fe x, y;
+    ge_affine(base_mul(s), &x, &y);
+    fe_tobytes(x, x_out);
+    fe_tobytes(y, y_out);
+}
+
 EXPORT void mko_pubkey_from_seed(const u8 seed[32], u8 pk[32]) {
     u8 s[32];
     oracle_init();

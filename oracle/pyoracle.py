@@ -40,6 +40,7 @@ def lib():
             "mko_secret_scalar": (None, [u8p, ctypes.c_void_p]),
             "mko_base_mul": (None, [u8p, ctypes.c_void_p]),
             "mko_pubkey_from_seed": (None, [u8p, ctypes.c_void_p]),
+            "mko_point_affine": (None, [u8p, ctypes.c_void_p, ctypes.c_void_p]),
             "mko_derive": (None, [u8p, ctypes.c_uint32, u64, u64, ctypes.c_void_p]),
             "mko_incremental": (None, [u8p, u64, u64, ctypes.c_void_p]),
             "mko_public_b64": (None, [u8p, ctypes.c_void_p]),
@@ -81,6 +82,14 @@ def base_mul(scalar: bytes) -> bytes:
     out = ctypes.create_string_buffer(32)
     lib().mko_base_mul(scalar, out)
     return out.raw
+
+
+def point_affine(scalar: int):
+    """(x, y) of scalar·B as integers (any 256-bit scalar)."""
+    x = ctypes.create_string_buffer(32)
+    y = ctypes.create_string_buffer(32)
+    lib().mko_point_affine(scalar.to_bytes(32, "little"), x, y)
+    return int.from_bytes(x.raw, "little"), int.from_bytes(y.raw, "little")
 
 
 def public_b64(pk: bytes) -> str:

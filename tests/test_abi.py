@@ -1,0 +1,79 @@
+"""The C-ABI library loads and exports every entry point that include/meikey_b200.h
+declares; argument checks and the no-device path return status codes (no GPU needed)."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from conftest import ROOT
+
+HEADER = os.path.join(ROOT, "include", "meikey_b200.h")
+
+
+def declared():
+    text = open(HEADER).read()
+    return sorted(set(re.findall(r"^MK_API\s+[\w\s\*]+?\b(mk_\w+)\(", text, re.M)))
+
+
+def test_header_declares_the_engine_surface():
+    names = declared()
+    for must in ["mk_ctx_create", "mk_ctx_destroy", "mk_job_prepare", "mk_job_launch", "mk_job_hits",
+                 "mk_keys_per_iter", "mk_derive", "mk_last_error"]:
+        assert must in names
+
+
+def test_library_exports_every_declared_symbol():
+    from meikey_b200 import _lib
+    lib = _lib.load()
+    raw = ctypes.CDLL(_lib.LIB_PATH)
+    bound = {n for n, _, _ in _lib.SIGNATURES}
+    for name in declared():
+        assert hasattr(raw, name), f"{name} declared but not exported"
+        assert name in bound, f"{name} not bound in meikey_b200/_lib.py"
+    assert lib.mk_abi_version() == 1
+
+
+def test_struct_layouts_match_header():
+    from meikey_b200 import _lib
+    assert ctypes.sizeof(_lib.Options) == 24
+    assert ctypes.sizeof(_lib.NeedleC) == 24
+    assert ctypes.sizeof(_lib.HitC) == 16
+    assert ctypes.sizeof(_lib.InfoC) == 4 * 6 + 16 + 96
+
+
+def test_bad_arguments_return_status():
+    from meikey_b200 import _lib
+    lib = _lib.load()
+    assert lib.mk_ctx_create(0, None, None) == _lib.ERR_BAD_ARG
+    assert lib.mk_ctx_info(None, None) == _lib.ERR_BAD_ARG
+    assert lib.mk_job_launch(None, 0, 1, None, None) == _lib.ERR_BAD_ARG
+    assert lib.mk_job_hits(None, None, 0, None, None) == _lib.ERR_BAD_ARG
+    assert lib.mk_ctx_sync(None) == _lib.ERR_BAD_ARG
+    assert lib.mk_keys_per_iter(None) == 0
+    buf = ctypes.create_string_buffer(8)
+    assert lib.mk_last_error(None, buf, 8) == _lib.OK and buf.value == b""
+
+
+def test_no_device_path_reports_an_error():
+    from meikey_b200 import _lib
+    import meikey_b200 as mk
+    lib = _lib.load()
+    if lib.mk_device_count() > 0:
+        pytest.skip("a CUDA device is present")
+    ptr = ctypes.c_void_p()
+    st = lib.mk_ctx_create(0, None, ctypes.byref(ptr))
+    assert st in (_lib.ERR_NO_DEVICE, _lib.ERR_DRIVER_NOT_FOUND)
+    assert not ptr
+    with pytest.raises(mk.GpuError) as e:
+        mk.Context()
+    assert e.value.status in (_lib.ERR_NO_DEVICE, _lib.ERR_DRIVER_NOT_FOUND)
+
+
+def test_missing_library_fails_loudly(tmp_path, monkeypatch):
+    """There is no CPU fallback: without the CUDA build the package refuses to run."""
+    from meikey_b200 import _lib
+    monkeypatch.setattr(_lib, "_lib", None)
+    monkeypatch.setattr(_lib, "LIB_PATH", str(tmp_path / "missing.so"))
+    with pytest.raises(OSError):
+        _lib.load()
