@@ -151,6 +151,19 @@ MK_API int mk_ctx_elapsed(mk_ctx* ctx, int from_slot, int to_slot, float* ms);
  * n full public keys (x sign included) of indices first..first+n-1 into host `out` (32·n bytes). */
 MK_API int mk_derive(mk_ctx* ctx, const uint8_t key[32], int seed_source, uint64_t first, uint64_t n, uint8_t* out);
 
+/* mk_derive that allocates nothing.  This entry point has no counterpart in the reference.
+ * It is for callers that must not allocate device memory while they run: a serving process
+ * that gave the device's memory to the comb table and job slots at start-up, or a host
+ * framework whose device memory belongs to its own pool; and cudaMalloc/cudaFree would also
+ * synchronize the device and stall every other job sharing it.  The device staging for the
+ * keys is a fixed 2 MiB array inside the library (held by every GPU that loads it until the
+ * process exits), so n is limited to 65536 keys; larger n returns MK_ERR_OUT_OF_RANGE.
+ * The first call on a device looks the array's device address up (make that first call
+ * before any stream capture).  All calls share the array: calls that overlap on the GPU,
+ * from any thread or context on the same device, race on it. */
+MK_API int mk_derive_noalloc(mk_ctx* ctx, const uint8_t key[32], int seed_source, uint64_t first, uint64_t n,
+                             uint8_t* out);
+
 /* Comb table entry (row, column) as 24 words (y+x, y-x, 2dxy; row 0 holds 2xy), for tests. */
 MK_API int mk_table_entry(mk_ctx* ctx, uint32_t row, uint64_t col, uint32_t out[24]);
 

@@ -105,7 +105,12 @@ SIGNATURES = [
     ("mk_ctx_work_per_key", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
                                            ctypes.POINTER(ctypes.c_double)]),
     ("mk_measure_imad_peak", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]),
+    ("mk_derive_noalloc", ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_uint64,
+                                         ctypes.c_uint64, ctypes.c_void_p]),
 ]
+
+# largest n of mk_derive_noalloc (its fixed device staging holds this many 32-byte keys)
+NOALLOC_MAX_KEYS = 1 << 16
 
 _lib = None
 

@@ -274,6 +274,35 @@ int mk_derive(mk_ctx* c, const uint8_t key[32], int seed_source, uint64_t first,
     return MK_OK;
 }
 
+// Same keys as mk_derive, with the device output staged in the library's fixed device
+// array instead of a cudaMalloc'd buffer: this call allocates nothing.  Every slot of the
+// staging that is copied back is written by the kernel first, so nothing has to be cleared.
+int mk_derive_noalloc(mk_ctx* c, const uint8_t key[32], int seed_source, uint64_t first, uint64_t n, uint8_t* out) {
+    if (!c || !key || (!out && n) || (seed_source != 0 && seed_source != 1)) return fail(c, MK_ERR_BAD_ARG, "bad argument");
+    if (n > mkb::NOALLOC_MAX_KEYS)
+        return fail(c, MK_ERR_OUT_OF_RANGE, "mk_derive_noalloc: n exceeds the fixed staging of 65536 keys");
+    if (n == 0) return MK_OK;
+    MK_CUDA(c, cudaSetDevice(c->device));
+    uint8_t* staging = nullptr;
+    MK_CUDA(c, mkb::noalloc_staging(c->device, &staging));
+    mkb::KeyLaunch L{};
+    L.table = c->table;
+    L.geom = c->geom;
+    for (int i = 0; i < 8; i++)
+        L.key[i] = (uint32_t)key[4 * i] | (uint32_t)key[4 * i + 1] << 8 | (uint32_t)key[4 * i + 2] << 16 | (uint32_t)key[4 * i + 3] << 24;
+    L.seed_src = (uint32_t)seed_source;
+    L.iters = 1;
+    L.base = first;
+    L.out = staging;
+    L.count = n;
+    uint64_t threads = (n + c->kpt - 1) / c->kpt;
+    uint32_t grid = (uint32_t)((threads + c->block - 1) / c->block);
+    MK_CUDA(c, mkb::launch_keys(L, true, c->kpt, c->block, grid, c->stream));
+    MK_CUDA(c, cudaMemcpyAsync(out, staging, n * 32, cudaMemcpyDeviceToHost, c->stream));
+    MK_CUDA(c, cudaStreamSynchronize(c->stream));
+    return MK_OK;
+}
+
 int mk_table_entry(mk_ctx* c, uint32_t row, uint64_t col, uint32_t out[24]) {
     if (!c || !out || row >= c->geom.rows || col >= c->geom.cols[row]) return fail(c, MK_ERR_BAD_ARG, "bad table entry");
     MK_CUDA(c, cudaSetDevice(c->device));

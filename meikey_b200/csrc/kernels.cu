@@ -644,3 +644,38 @@ cudaError_t measure_imad(int sms, cudaStream_t st, double* mads_per_s) {
 }
 
 }  // namespace mkb
+
+// ---------------------------------------------------------------------------
+// Derive without allocation: fixed device staging for mk_derive_noalloc
+// ---------------------------------------------------------------------------
+
+#include <mutex>
+
+namespace mkb {
+
+// Device-side staging of the public keys written by mk_derive_noalloc: 65536 keys of 32
+// bytes (2 MiB).  It is a file-scope device array, so every GPU that loads this library
+// holds it until the process exits, and no call has to allocate device memory for it.
+static __device__ __align__(256) uint8_t g_noalloc_pubkeys[NOALLOC_MAX_KEYS * 32];
+
+// Device address of g_noalloc_pubkeys on `device` (which must be current).  The name of
+// the array in host code is only a host-side stand-in; the address is looked up once per
+// device with cudaGetSymbolAddress and cached.
+cudaError_t noalloc_staging(int device, uint8_t** ptr) {
+    static std::mutex mu;
+    static uint8_t* addr[64];
+    static bool known[64];
+    if (device < 0 || device >= 64) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!known[device]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_pubkeys);
+        if (e != cudaSuccess) return e;
+        addr[device] = static_cast<uint8_t*>(p);
+        known[device] = true;
+    }
+    *ptr = addr[device];
+    return cudaSuccess;
+}
+
+}  // namespace mkb

@@ -87,6 +87,17 @@ class Context:
         _check(self._lib, self._ptr, self._lib.mk_derive(self._ptr, bytes(key), source, first, n, out))
         return out.raw
 
+    def derive_noalloc(self, key: bytes, source: int, first: int, n: int) -> bytes:
+        """As derive, through the entry point that allocates no device memory (n <= 65536).
+
+        For callers that must not allocate device memory mid-run (a serving process whose
+        device memory is committed at start-up, or one whose memory a host framework's pool
+        owns); the first call on a device should come before any stream capture, and calls
+        that overlap on the GPU share, and race on, the library's fixed staging array."""
+        out = ctypes.create_string_buffer(32 * n)
+        _check(self._lib, self._ptr, self._lib.mk_derive_noalloc(self._ptr, bytes(key), source, first, n, out))
+        return out.raw
+
     def table_entry(self, row: int, col: int) -> List[int]:
         out = (ctypes.c_uint32 * 24)()
         _check(self._lib, self._ptr, self._lib.mk_table_entry(self._ptr, row, col, out))
