@@ -1,14 +1,22 @@
 """Benchmark of the candidate-key search path (one JSON line on rank 0).
 
-Workload (the reference's throughput configuration, synthetic inputs): secure-path seeds
-from ChaCha20 with key SHA-256(u64 7 little-endian), a case-sensitive 7-character contains
-needle drawn uniformly from the base64 alphabet with numpy.random.default_rng(7), 2^34
-candidates in total.  A step is one launch over >= 2^30 consecutive candidate indices;
-the default 16 steps cover 2^34.  Multi-GPU: one process per GPU (torchrun), each rank
-searches its own index range (rank·2^56 ...), so the work is weakly scaled with no
-data-path collective; timing is the max over ranks.
+Default workload (the reference's throughput configuration, synthetic inputs): secure-path
+seeds from ChaCha20 with key SHA-256(u64 7 little-endian), a case-sensitive 7-character
+contains needle drawn uniformly from the base64 alphabet with numpy.random.default_rng(7),
+2^34 candidates in total.  A step is one launch over >= 2^30 consecutive candidate indices;
+the default 16 steps cover 2^34.
+
+--workload incremental: the low-security incremental path.  The start scalar is
+clamp(SHA-512(ChaCha20 seed 0 of key SHA-256(u64 11))), index k is the point (s0 + k)·B,
+the needle is a case-sensitive 6-character suffix drawn with numpy.random.default_rng(11),
+2^32 candidates (16 steps of >= 2^28).
+
+Multi-GPU: one process per GPU (torchrun), each rank searches its own index range
+(rank·2^56 ...), so the work is weakly scaled with no data-path collective; timing is the
+max over ranks.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload secure|incremental]
 """
 import argparse
 import hashlib
@@ -27,18 +35,57 @@ sys.path.insert(0, ROOT)
 METRIC = "keys/s on 1 B200 (bit-exact pubkeys), % int-MAD peak; multi-job p50/p99"
 UNIT = "keys/s"
 ALPHABET = "ABCDEFGHIJKLMNOPQRSTUVWXYZabcdefghijklmnopqrstuvwxyz0123456789+/"
-TOTAL_CANDIDATES = 1 << 34
-STEP_CANDIDATES = 1 << 30
+# per workload: total candidates, candidates per step, seed source, generator seed, needle length, mode
+WORKLOADS = {
+    "secure": {"total": 1 << 34, "step": 1 << 30, "source": 0, "seed": 7, "length": 7, "mode": "contains"},
+    "incremental": {"total": 1 << 32, "step": 1 << 28, "source": 2, "seed": 11, "length": 6, "mode": "suffix"},
+}
 
 
-def workload_key() -> bytes:
-    return hashlib.sha256((7).to_bytes(8, "little")).digest()
+def chacha20_seed0(key: bytes) -> bytes:
+    """The first 32 bytes of the ChaCha20 keystream (RFC 8439 block 0, nonce 0)."""
+    def rotl(x, n):
+        return ((x << n) | (x >> (32 - n))) & 0xFFFFFFFF
+
+    def qr(s, a, b, c, d):
+        s[a] = (s[a] + s[b]) & 0xFFFFFFFF; s[d] = rotl(s[d] ^ s[a], 16)
+        s[c] = (s[c] + s[d]) & 0xFFFFFFFF; s[b] = rotl(s[b] ^ s[c], 12)
+        s[a] = (s[a] + s[b]) & 0xFFFFFFFF; s[d] = rotl(s[d] ^ s[a], 8)
+        s[c] = (s[c] + s[d]) & 0xFFFFFFFF; s[b] = rotl(s[b] ^ s[c], 7)
+    init = [0x61707865, 0x3320646E, 0x79622D32, 0x6B206574]
+    init += [int.from_bytes(key[4 * i:4 * i + 4], "little") for i in range(8)] + [0, 0, 0, 0]
+    s = list(init)
+    for _ in range(10):
+        qr(s, 0, 4, 8, 12); qr(s, 1, 5, 9, 13); qr(s, 2, 6, 10, 14); qr(s, 3, 7, 11, 15)
+        qr(s, 0, 5, 10, 15); qr(s, 1, 6, 11, 12); qr(s, 2, 7, 8, 13); qr(s, 3, 4, 9, 14)
+    return b"".join(((s[i] + init[i]) & 0xFFFFFFFF).to_bytes(4, "little") for i in range(8))
 
 
-def workload_needle() -> str:
+def workload_key(name: str = "secure") -> bytes:
+    """ChaCha20 key SHA-256(u64 seed); the incremental workload's key is its start scalar
+    clamp(SHA-512(ChaCha20 seed 0 of that key))."""
+    w = WORKLOADS[name]
+    key = hashlib.sha256(w["seed"].to_bytes(8, "little")).digest()
+    if w["source"] != 2:
+        return key
+    h = bytearray(hashlib.sha512(chacha20_seed0(key)).digest()[:32])
+    h[0] &= 248
+    h[31] &= 127
+    h[31] |= 64
+    return bytes(h)
+
+
+def workload_needle(name: str = "secure") -> str:
     import numpy as np
-    rng = np.random.default_rng(7)
-    return "".join(ALPHABET[int(i)] for i in rng.integers(0, 64, 7))
+    w = WORKLOADS[name]
+    rng = np.random.default_rng(w["seed"])
+    return "".join(ALPHABET[int(i)] for i in rng.integers(0, 64, w["length"]))
+
+
+def workload_needles(name: str = "secure"):
+    import meikey_b200 as mk
+    n = workload_needle(name)
+    return [mk.Needle.suffix(n) if WORKLOADS[name]["mode"] == "suffix" else mk.Needle.contains(n)]
 
 
 class ClockSampler:
@@ -137,12 +184,17 @@ class Dist:
 # ---------------------------------------------------------------------------
 
 class CpuBaseline:
-    def __init__(self):
+    """The reference's kernel built for the CPU (secure path), else the C oracle port (and
+    always the port for the incremental path, which has no reference implementation)."""
+
+    def __init__(self, workload: str = "secure"):
         from oracle import pyoracle
         self.po = pyoracle
         self.threads = os.cpu_count() or 1
+        self.source = WORKLOADS[workload]["source"]
+        self.mode = 1 if WORKLOADS[workload]["mode"] == "suffix" else 0
         variants = [p for p in pyoracle.ref_variants() if "f8_b32" in p] or pyoracle.ref_variants()
-        if variants:
+        if variants and self.source == 0:
             self.kind = "reference"
             self.ref = pyoracle.RefKernel(variants[0])
             self.width = 16
@@ -152,7 +204,7 @@ class CpuBaseline:
         else:
             self.kind = "port"
             self.ref = None
-            self.what = f"C oracle restatement of the path on {self.threads} threads"
+            self.what = f"C oracle restatement of the path (one base-point multiply per key) on {self.threads} threads"
 
     def run(self, key: bytes, needle: str, seconds: float, base: int = 0):
         """keys/s over a sample of about `seconds` of work on all threads."""
@@ -176,7 +228,7 @@ class CpuBaseline:
             keys = self.threads * per_call * iters
         else:
             def job(t, n):
-                self.po.search(key, 0, base + t * (1 << 40), n, nb, len(nb), False, 0, threads=1)
+                self.po.search(key, self.source, base + t * (1 << 40), n, nb, len(nb), False, self.mode, threads=1)
             t0 = time.perf_counter()
             job(0, 2000)
             per_key = max((time.perf_counter() - t0) / 2000, 1e-7)
@@ -197,8 +249,8 @@ def run_reference(args):
     world, rank, local = dist_env()
     if rank != 0:
         return 0
-    key, needle = workload_key(), workload_needle()
-    cpu = CpuBaseline()
+    key, needle = workload_key(args.workload), workload_needle(args.workload)
+    cpu = CpuBaseline(args.workload)
     per_step = args.ref_step_seconds
     for _ in range(args.warmup):
         cpu.run(key, needle, per_step / 4)
@@ -214,7 +266,7 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * dt / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-        "config": workload_config(None),
+        "config": workload_config(args.workload, None),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cpu.threads, "kind": cpu.kind,
                          "sample": f"{keys} candidates over {args.steps} steps; {cpu.what}"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -223,13 +275,22 @@ def run_reference(args):
     return 0
 
 
-def workload_config(ctx, step_candidates=None, steps=None):
-    cfg = {
-        "workload": "secure-path throughput: ChaCha20 seeds (key SHA-256(u64 7)), SHA-512, clamp, "
-                    "comb multiply, pooled inversion, base64, case-sensitive 7-char contains "
-                    f"'{workload_needle()}' (numpy default_rng(7)); 2^34 candidates",
-        "candidates_total": TOTAL_CANDIDATES,
-    }
+def workload_config(workload, ctx, step_candidates=None, steps=None):
+    if workload == "incremental":
+        cfg = {
+            "workload": "incremental (low-security) path: s0 = clamp(SHA-512(ChaCha20 seed 0 of key "
+                        "SHA-256(u64 11))), P_k = P_0 + k*B by mixed additions, pooled inversion, base64, "
+                        f"case-sensitive 6-char suffix '{workload_needle(workload)}' (numpy default_rng(11)); "
+                        "2^32 candidates",
+            "candidates_total": WORKLOADS[workload]["total"],
+        }
+    else:
+        cfg = {
+            "workload": "secure-path throughput: ChaCha20 seeds (key SHA-256(u64 7)), SHA-512, clamp, "
+                        "comb multiply, pooled inversion, base64, case-sensitive 7-char contains "
+                        f"'{workload_needle(workload)}' (numpy default_rng(7)); 2^34 candidates",
+            "candidates_total": WORKLOADS[workload]["total"],
+        }
     if ctx is not None:
         info = ctx.info
         cfg.update({
@@ -241,14 +302,18 @@ def workload_config(ctx, step_candidates=None, steps=None):
             "block": info["block"],
             "grid": info["grid"],
             "inversion_batch": info["keys_per_thread"] * info["block"] // 32,
-            "l2": "inputs larger than L2: random gathers from the comb table in HBM",
+            "l2": ("no memory-resident inputs: each thread steps its own point, the 14 KB step tables "
+                   "stay on chip" if workload == "incremental" else
+                   "inputs larger than L2: random gathers from the comb table in HBM"),
             "parallelism": "one process per GPU, disjoint index ranges (rank * 2^56), no collective",
         })
     return cfg
 
 
-def traffic_per_key():
-    path = os.path.join(ROOT, "profiles", "k_search_dram.json")
+def traffic_per_key(workload):
+    """DRAM bytes per key of the search kernel from the committed ncu summary of this workload."""
+    path = os.path.join(ROOT, "profiles", "k_search_dram.json" if workload == "secure" else
+                        f"k_search_{workload}_dram.json")
     try:
         with open(path) as f:
             return json.load(f).get("dram_bytes_per_key")
@@ -260,16 +325,17 @@ def run_ours(args):
     world, rank, local = dist_env()
     dist = Dist(world, local)
     import meikey_b200 as mk
-    key, needle = workload_key(), workload_needle()
+    wl = WORKLOADS[args.workload]
+    key, needle, source = workload_key(args.workload), workload_needle(args.workload), wl["source"]
     ctx = mk.Context(device=local, table_rows=args.rows, keys_per_thread=args.kpt, block=args.block,
                      self_check=True)
     kpi = ctx.keys_per_iter
-    iters = math.ceil(args.step_candidates / kpi)
+    iters = math.ceil((args.step_candidates or wl["step"]) / kpi)
     step_keys = kpi * iters
     rank_base = rank << 56
-    peak = ctx.measure_imad_peak()
-    field_muls, mads_per_key = ctx.work_per_key()
-    job = ctx.job(key, mk.SEED_CHACHA20, [mk.Needle.contains(needle)])
+    peak, peak_lo = ctx.measure_mad_peaks()
+    field_muls, mads_per_key = ctx.work_per_key(source)
+    job = ctx.job(key, source, workload_needles(args.workload))
     # warm-up
     for w in range(args.warmup):
         job.enqueue(rank_base + w * step_keys, iters)
@@ -293,17 +359,19 @@ def run_ours(args):
     value = keys_all / (ms / 1000.0)
     per_gpu = step_keys * args.steps / (ms_local / 1000.0)
     # end to end through the public API: prepare (H2D of key + compiled needle), launch,
-    # read the job state and hits back (D2H), confirm hits on the host
+    # read the job state and hits back (D2H), confirm every hit on the host
     e2e_steps = args.e2e_steps or args.steps
     h2d = d2h = 0
-    found = 0
+    found = confirmed = 0
     dist.barrier()
     t0 = time.perf_counter()
     for s in range(e2e_steps):
-        with ctx.job(key, mk.SEED_CHACHA20, [mk.Needle.contains(needle)]) as j:
+        with ctx.job(key, source, workload_needles(args.workload)) as j:
             j.launch(first + (args.steps + s) * step_keys, iters)
             hits, total = j.hits()
             found += total
+            for index, nd in hits:
+                confirmed += j.confirm(index, nd)[0]
             a, b = j.io_bytes()
             h2d += a
             d2h += b
@@ -315,29 +383,33 @@ def run_ours(args):
     line = None
     if rank == 0:
         achieved = mads_per_key * per_gpu / 1e12
-        tpk = traffic_per_key()
+        tpk = traffic_per_key(args.workload)
         roofline = {
             "bound": "int_mad", "achieved": achieved, "peak": peak / 1e12, "unit": "Tmad/s",
             "frac": achieved / (peak / 1e12) if peak else None,
             "traffic": tpk * step_keys if tpk else None,
-            "peak_source": "measured live: mad.lo.u32 independent chains at full occupancy (mk_measure_imad_peak)",
+            "peak_source": "measured live: rows of mad.lo.cc/madc.hi.cc carry chains shaped like the field "
+                           "multiply, independent accumulators, full occupancy (mk_measure_mad_peaks)",
+            "peak_mad_lo": peak_lo / 1e12,
+            "frac_of_mad_lo": achieved / (peak_lo / 1e12) if peak_lo else None,
             "work_per_key": {"field_muls": field_muls, "int_mads": mads_per_key},
             "kernel_ms_per_launch": ms_local / args.steps,
         }
-        cfg = workload_config(ctx, step_keys, args.steps)
+        cfg = workload_config(args.workload, ctx, step_keys, args.steps)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u32", "data": "synthetic", "config": cfg, "clocks": clk,
             "gpu_launches": args.steps,
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d // e2e_steps,
-                    "d2h_bytes_per_step": d2h // e2e_steps, "steps": e2e_steps, "hits_found": found},
+                    "d2h_bytes_per_step": d2h // e2e_steps, "steps": e2e_steps, "candidates": found,
+                    "confirmed_on_host": confirmed},
             "roofline": roofline,
             "device": ctx_info["name"],
         }
     ctx.close()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = CpuBaseline()
+        cpu = CpuBaseline(args.workload)
         rate, keys = cpu.run(key, needle, args.cpu_seconds)
         line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cpu.threads, "kind": cpu.kind,
                                 "sample": f"{keys} candidates of the same workload; {cpu.what}"}
@@ -357,8 +429,10 @@ def main():
     ap.add_argument("--kpt", type=int, default=16, help="keys per thread")
     ap.add_argument("--block", type=int, default=512)
     ap.add_argument("--e2e-steps", type=int, default=0, help="end-to-end steps (default: --steps)")
-    ap.add_argument("--step-candidates", type=int, default=STEP_CANDIDATES,
-                    help="candidates per step (default 2^30; smaller only for profiling captures)")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="secure")
+    ap.add_argument("--step-candidates", type=int, default=0,
+                    help="candidates per step (default 2^30 secure, 2^28 incremental; smaller only for "
+                         "profiling captures)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample length")
     ap.add_argument("--ref-step-seconds", type=float, default=2.0, help="reference arm: seconds per step")
     ap.add_argument("--no-cpu-baseline", action="store_true")

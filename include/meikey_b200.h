@@ -14,6 +14,11 @@
  *                     (RFC 8439 block function, 64-bit counter, stream 0), key = `key`
  *   MK_SEED_COUNTER   seed(i) = key with i added to its last 8 bytes (little-endian)
  * The public key of a seed is the Ed25519 public key: compress(clamp(SHA-512(seed)[0..32])·B).
+ *   MK_SEED_INCREMENTAL  the low-security incremental path: `key` is a little-endian scalar
+ *                     s0 below 2^255 (e.g. a clamped SHA-512 of one seed) and index i stands
+ *                     for the scalar s0 + i itself, public key compress((s0 + i)·B), so
+ *                     consecutive keys are consecutive points P_i = P_0 + i·B.  The reference
+ *                     has no GPU kernel for it; the host confirms a hit from s0 + i.
  */
 #ifndef MEIKEY_B200_H
 #define MEIKEY_B200_H
@@ -52,7 +57,7 @@ enum mk_status {
 };
 
 /* seed sources (SeedSource, src/model/search.rs:27-36) */
-enum mk_seed_source { MK_SEED_CHACHA20 = 0, MK_SEED_COUNTER = 1 };
+enum mk_seed_source { MK_SEED_CHACHA20 = 0, MK_SEED_COUNTER = 1, MK_SEED_INCREMENTAL = 2 };
 
 /* match modes (kernel.cu MODE_CONTAINS / MODE_SUFFIX / MODE_REGEX, src/service/gpu.rs:610-616) */
 enum mk_mode { MK_MODE_CONTAINS = 0, MK_MODE_SUFFIX = 1, MK_MODE_REGEX = 2 };
@@ -105,6 +110,7 @@ typedef struct mk_info {
 
 typedef struct mk_ctx mk_ctx;
 typedef struct mk_job mk_job;
+typedef struct mk_graph mk_graph;
 
 /* Library ABI version (MK_ABI_VERSION). */
 MK_API uint32_t mk_abi_version(void);
@@ -139,6 +145,31 @@ MK_API int mk_job_launch(mk_job* job, uint64_t base, uint32_t iters, int* found,
  * number kept when the device ring overflowed (then MK_ERR_HIT_RING_FULL is returned). */
 MK_API int mk_job_hits(mk_job* job, mk_hit* out, uint32_t cap, uint32_t* written, uint64_t* total);
 
+/* Replaces the job's needles between launches (same rules as mk_job_prepare; waits for the
+ * job's queued launches first).  Text needles are re-packed into the existing device copy
+ * without allocating; regex needles get fresh device tables.  Hits of later launches carry
+ * positions in the new array.  The reference rebuilds a Launch instead (gpu.rs:836-857). */
+MK_API int mk_job_update(mk_job* job, const mk_needle* needles, uint32_t n_needles);
+
+/* CUDA graph of `launches` consecutive search launches of `iters` iterations each (the job
+ * word is reset once at the start; hits of all launches accumulate in the job's ring).
+ * mk_graph_launch replays it over base .. base + launches·iters·keys_per_iter - 1, waits and
+ * reports like mk_job_launch (hits through mk_job_hits); mk_graph_enqueue only queues it.
+ * The reference launches each range from the host loop instead (gpu.rs:917-971). */
+MK_API int mk_job_graph_create(mk_job* job, uint32_t iters, uint32_t launches, mk_graph** out);
+MK_API int mk_graph_launch(mk_graph* graph, uint64_t base, int* found, uint64_t* index);
+MK_API int mk_graph_enqueue(mk_graph* graph, uint64_t base);
+MK_API void mk_graph_destroy(mk_graph* graph);
+
+/* The host confirmation of a candidate (src/service/gpu.rs:973-996, confirm): re-derives
+ * index `index` of the job's key stream on the CPU — the seed and its Ed25519 public key, or
+ * for MK_SEED_INCREMENTAL the scalar s0 + index and (s0 + index)·B — and tests needle
+ * `needle` against the full key (x sign known).  Writes the public key and the secret (the
+ * 32-byte seed, or the 32-byte little-endian scalar) and sets *matched to 1 when the key
+ * matches; a candidate that only matched through the other x sign gives *matched = 0. */
+MK_API int mk_job_confirm(mk_job* job, uint64_t index, uint32_t needle, uint8_t pk[32], uint8_t secret[32],
+                          int* matched);
+
 /* Asynchronous form for timing: enqueue one launch on the context's stream without
  * waiting; mk_ctx_sync waits for all queued work. */
 MK_API int mk_job_enqueue(mk_job* job, uint64_t base, uint32_t iters);
@@ -171,14 +202,19 @@ MK_API int mk_table_entry(mk_ctx* ctx, uint32_t row, uint64_t col, uint32_t out[
  * compiled needles, job state and hit records), for end-to-end accounting. */
 MK_API int mk_job_io_bytes(const mk_job* job, uint64_t* h2d, uint64_t* d2h);
 
-/* Field multiplications and 32-bit integer multiply-adds per key of the configured
- * search kernel (the algorithmic count: comb additions, batch-inversion share, compression). */
-MK_API int mk_ctx_work_per_key(const mk_ctx* ctx, double* field_muls, double* int_mads);
+/* Field multiplications and 32-bit integer multiply-adds per key of the configured search
+ * kernel for a seed source (the algorithmic count: comb additions, or the incremental
+ * source's point additions, batch-inversion share, compression). */
+MK_API int mk_ctx_work_per_key(const mk_ctx* ctx, int seed_source, double* field_muls, double* int_mads);
 
-/* Measured peak of 32-bit integer multiply-adds (mad.lo.u32, independent chains, full
- * occupancy, best of three bounded runs of about 20 ms) on the context's device, in MADs/s.
- * This is the denominator of the int-MAD roofline (the reference reports none). */
-MK_API int mk_measure_imad_peak(mk_ctx* ctx, double* mads_per_s);
+/* Measured peaks of 32-bit integer multiply-adds on the context's device, in MADs/s, each
+ * the best of three bounded runs of 10-30 ms at full occupancy with no memory traffic:
+ *   *chain_per_s  rows of a schoolbook product as the field multiply issues them
+ *                 (mad.lo.cc/madc.lo.cc then madc.hi.cc carry chains, 8 lo + 8 hi per row);
+ *                 the denominator of the int-MAD roofline;
+ *   *lo_per_s     plain mad.lo.u32 on independent registers (the low-half multiply rate).
+ * The reference reports no roofline. */
+MK_API int mk_measure_mad_peaks(mk_ctx* ctx, double* chain_per_s, double* lo_per_s);
 
 #ifdef __cplusplus
 }

@@ -33,6 +33,7 @@ STATUS_NAMES = {
 
 SEED_CHACHA20 = 0
 SEED_COUNTER = 1
+SEED_INCREMENTAL = 2
 MODE_CONTAINS = 0
 MODE_SUFFIX = 1
 MODE_REGEX = 2
@@ -92,6 +93,15 @@ SIGNATURES = [
                                      ctypes.POINTER(ctypes.c_uint64)]),
     ("mk_job_hits", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(HitC), ctypes.c_uint32,
                                    ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint64)]),
+    ("mk_job_update", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(NeedleC), ctypes.c_uint32]),
+    ("mk_job_graph_create", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_uint32,
+                                           ctypes.POINTER(ctypes.c_void_p)]),
+    ("mk_graph_launch", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(ctypes.c_int),
+                                       ctypes.POINTER(ctypes.c_uint64)]),
+    ("mk_graph_enqueue", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64]),
+    ("mk_graph_destroy", None, [ctypes.c_void_p]),
+    ("mk_job_confirm", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_void_p,
+                                      ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]),
     ("mk_job_enqueue", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32]),
     ("mk_ctx_sync", ctypes.c_int, [ctypes.c_void_p]),
     ("mk_ctx_record", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
@@ -102,9 +112,10 @@ SIGNATURES = [
                                       ctypes.POINTER(ctypes.c_uint32)]),
     ("mk_job_io_bytes", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64),
                                        ctypes.POINTER(ctypes.c_uint64)]),
-    ("mk_ctx_work_per_key", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
+    ("mk_ctx_work_per_key", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
                                            ctypes.POINTER(ctypes.c_double)]),
-    ("mk_measure_imad_peak", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]),
+    ("mk_measure_mad_peaks", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
+                                            ctypes.POINTER(ctypes.c_double)]),
     ("mk_derive_noalloc", ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_uint64,
                                          ctypes.c_uint64, ctypes.c_void_p]),
 ]

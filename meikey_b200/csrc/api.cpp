@@ -8,6 +8,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <memory>
 #include <new>
 #include <string>
 #include <vector>
@@ -25,6 +26,8 @@ struct mk_ctx {
     mk_info info{};
     CombGeom geom{};
     uint4* table = nullptr;
+    uint4* incr = nullptr;           // incremental source: window table then step table
+    uint32_t delta[24] = {};         // keys_per_iter·B (table form)
     uint32_t kpt = 8, block = 256, grid = 0;
     uint32_t hit_capacity = 1u << 16;
     std::string err;
@@ -45,6 +48,18 @@ struct mk_job {
     std::vector<mk_hit> last;
     uint32_t last_total = 0;
     uint64_t h2d = 0, d2h = 0;  // bytes copied for this job
+};
+
+struct mk_graph {
+    mk_job* job = nullptr;
+    uint32_t iters = 0;
+    uint64_t span = 0;  // keys of one launch
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<cudaGraphNode_t> nodes;
+    std::vector<mkb::KeyLaunch> params;
+    const void* func = nullptr;
+    size_t dyn = 0;
 };
 
 namespace {
@@ -110,20 +125,43 @@ bool make_geometry(uint32_t rows, CombGeom& g) {
     return off == 251;
 }
 
+// Public key of index `index` of a job's key stream on the host (the confirmation path).
+bool host_public_key(const uint8_t key[32], int source, uint64_t index, uint8_t pk[32]) {
+    if (source == MK_SEED_INCREMENTAL) {
+        uint8_t s[32];
+        if (!mkh25519::incremental_scalar(key, index, s)) return false;
+        mkh25519::scalar_public_key(s, pk);
+        return true;
+    }
+    uint8_t seed[32];
+    mkh25519::seed_of(key, source, index, seed);
+    mkh25519::public_key(seed, pk);
+    return true;
+}
+
+// KeyLaunch fields of the incremental source for a launch starting at index `base`.
+void set_incremental(const mk_ctx* c, const uint8_t s0[32], uint64_t base, mkb::KeyLaunch& L) {
+    uint8_t s[32];
+    mkh25519::incremental_scalar(s0, base, s);
+    mkh25519::scalar_point_words(s, L.start);
+    memcpy(L.delta, c->delta, sizeof L.delta);
+    L.incr = c->incr;
+}
+
 int self_check(mk_ctx* c) {
-    // both seed sources, an odd first index (seed from the second half of a block)
+    // every seed source, an odd first index (seed from the second half of a block)
     const uint64_t n = 257;
     std::vector<uint8_t> got(32 * n);
-    for (int src = 0; src < 2; src++) {
+    for (int src = 0; src < 3; src++) {
         uint8_t key[32];
         for (int i = 0; i < 32; i++) key[i] = (uint8_t)(0x5a ^ (i * 37 + src * 101));
+        key[31] &= 0x7f;  // incremental scalars start below 2^255
         uint64_t first = 0x123456789abull | 1;
         int st = mk_derive(c, key, src, first, n, got.data());
         if (st) return st;
         for (uint64_t i = 0; i < n; i += (i < 8 ? 1 : 31)) {
-            uint8_t seed[32], pk[32];
-            mkh25519::seed_of(key, src, first + i, seed);
-            mkh25519::public_key(seed, pk);
+            uint8_t pk[32];
+            host_public_key(key, src, first + i, pk);
             if (memcmp(pk, &got[32 * i], 32) != 0)
                 return fail(c, MK_ERR_SELF_CHECK, "GPU public keys differ from the host derivation");
         }
@@ -180,7 +218,7 @@ int mk_ctx_create(int device, const mk_options* options, mk_ctx** out) {
     cudaDeviceProp prop;
     MK_CUDA(c, cudaGetDeviceProperties(&prop, device));
     int occ = 0;
-    MK_CUDA(c, mkb::keys_occupancy(false, c->kpt, c->block, &occ));
+    MK_CUDA(c, mkb::keys_occupancy(false, false, c->kpt, c->block, &occ));
     if (occ < 1) return fail(c, MK_ERR_NOT_BUILT, "kernel does not fit on this device");
     uint32_t per_sm = o.blocks_per_sm ? std::min<uint32_t>(o.blocks_per_sm, (uint32_t)occ) : (uint32_t)occ;
     c->grid = (uint32_t)prop.multiProcessorCount * per_sm;
@@ -203,6 +241,22 @@ int mk_ctx_create(int device, const mk_options* options, mk_ctx** out) {
     }
     MK_CUDA(c, cudaStreamSynchronize(c->stream));
     cudaFree(d_pts);
+    // incremental source: j·16^w·B (w < 8, j < 16), then j·B (j < 16), in the table form
+    {
+        std::vector<uint32_t> words((size_t)mkb::INCR_ENTRIES * mkb::ENTRY_WORDS);
+        for (int w = 0; w < mkb::INCR_WINDOWS; w++)
+            for (int j = 0; j < 16; j++)
+                mkh25519::niels_of_multiple((uint64_t)j << (4 * w), &words[(size_t)(w * 16 + j) * mkb::ENTRY_WORDS]);
+        for (int j = 0; j < mkb::INCR_STEPS; j++)
+            mkh25519::niels_of_multiple((uint64_t)j,
+                                        &words[(size_t)(mkb::INCR_WINDOWS * 16 + j) * mkb::ENTRY_WORDS]);
+        if (cudaMalloc(&c->incr, words.size() * 4) != cudaSuccess) {
+            c->incr = nullptr;
+            return fail(c, MK_ERR_OUT_OF_MEMORY, "incremental table allocation failed");
+        }
+        MK_CUDA(c, cudaMemcpy(c->incr, words.data(), words.size() * 4, cudaMemcpyHostToDevice));
+        mkh25519::niels_of_multiple((uint64_t)c->grid * (c->block - 32) * c->kpt, c->delta);
+    }
     // info
     mk_info& in = c->info;
     in.device = device;
@@ -227,6 +281,7 @@ void mk_ctx_destroy(mk_ctx* c) {
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->table) cudaFree(c->table);
+    if (c->incr) cudaFree(c->incr);
     for (auto& ev : c->ev)
         if (ev) cudaEventDestroy(ev);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -241,8 +296,17 @@ int mk_ctx_info(const mk_ctx* c, mk_info* out) {
 
 uint64_t mk_keys_per_iter(const mk_ctx* c) { return c ? c->info.keys_per_iter : 0; }
 
+// Sources 0..2; the incremental source takes a scalar below 2^255 as its key.
+static int check_source(mk_ctx* c, const uint8_t key[32], int seed_source) {
+    if (seed_source < MK_SEED_CHACHA20 || seed_source > MK_SEED_INCREMENTAL) return fail(c, MK_ERR_BAD_ARG, "unknown seed source");
+    if (seed_source == MK_SEED_INCREMENTAL && (key[31] & 0x80))
+        return fail(c, MK_ERR_BAD_ARG, "incremental start scalar must be below 2^255");
+    return MK_OK;
+}
+
 int mk_derive(mk_ctx* c, const uint8_t key[32], int seed_source, uint64_t first, uint64_t n, uint8_t* out) {
-    if (!c || !key || (!out && n) || (seed_source != 0 && seed_source != 1)) return fail(c, MK_ERR_BAD_ARG, "bad argument");
+    if (!c || !key || (!out && n)) return fail(c, MK_ERR_BAD_ARG, "bad argument");
+    if (int st = check_source(c, key, seed_source)) return st;
     if (n == 0) return MK_OK;
     MK_CUDA(c, cudaSetDevice(c->device));
     const uint64_t per_launch = 1ull << 22;
@@ -260,6 +324,7 @@ int mk_derive(mk_ctx* c, const uint8_t key[32], int seed_source, uint64_t first,
         L.base = first + done;
         L.out = d_out;
         L.count = cnt;
+        if (seed_source == MK_SEED_INCREMENTAL) set_incremental(c, key, L.base, L);
         uint64_t threads = (cnt + c->kpt - 1) / c->kpt;
         uint32_t grid = (uint32_t)((threads + c->block - 1) / c->block);
         cudaError_t e = mkb::launch_keys(L, true, c->kpt, c->block, grid, c->stream);
@@ -310,31 +375,16 @@ int mk_table_entry(mk_ctx* c, uint32_t row, uint64_t col, uint32_t out[24]) {
     return MK_OK;
 }
 
-int mk_job_prepare(mk_ctx* c, const uint8_t key[32], int seed_source, const mk_needle* needles, uint32_t n_needles,
-                   int stop_on_hit, mk_job** out) {
-    if (!c || !key || !out || (n_needles && !needles) || (seed_source != 0 && seed_source != 1))
-        return fail(c, MK_ERR_BAD_ARG, "bad argument");
+// Compiles needles into a MatchSet on the host (src/service/gpu.rs:618-660 Needle::new,
+// dfa.rs:189-200): text needles become bit ranges of the shift-and state (a needle never
+// straddles a 64-bit word; fold lowercases the needle and accepts the uppercase value too),
+// DFA tables are validated and kept for upload.  No device work.
+static int pack_needles(mk_ctx* c, const mk_needle* needles, uint32_t n_needles, mkb::MatchSet& ms,
+                        std::vector<mkh25519::Needle>& hosts) {
+    if (n_needles && !needles) return fail(c, MK_ERR_BAD_ARG, "bad argument");
     if (n_needles > (uint32_t)mkb::MAX_NEEDLES) return fail(c, MK_ERR_BAD_ARG, "too many needles");
-    *out = nullptr;
-    MK_CUDA(c, cudaSetDevice(c->device));
-    mkb::MatchSet* ms = new (std::nothrow) mkb::MatchSet;
-    if (!ms) return fail(c, MK_ERR_OUT_OF_MEMORY, "host allocation");
-    memset(ms, 0, sizeof *ms);
-    mk_job* j = new (std::nothrow) mk_job;
-    if (!j) {
-        delete ms;
-        return fail(c, MK_ERR_OUT_OF_MEMORY, "host allocation");
-    }
-    j->ctx = c;
-    memcpy(j->key, key, 32);
-    j->source = seed_source;
-    j->stop_on_hit = stop_on_hit;
-    j->cap = c->hit_capacity;
-    auto bail = [&](int code, const std::string& msg) {
-        delete ms;
-        mk_job_destroy(j);
-        return fail(c, code, msg);
-    };
+    memset(&ms, 0, sizeof ms);
+    hosts.clear();
     uint32_t bit = 0;  // next free bit in the shift-and state
     for (uint32_t i = 0; i < n_needles; i++) {
         const mk_needle& nd = needles[i];
@@ -343,73 +393,123 @@ int mk_job_prepare(mk_ctx* c, const uint8_t key[32], int seed_source, const mk_n
         h.fold = nd.fold != 0;
         h.len = nd.len;
         if (nd.mode == MK_MODE_REGEX) {
-            if (nd.len == 0 || nd.len > 65535 || !nd.bytes) return bail(MK_ERR_BAD_ARG, "bad DFA table");
+            if (nd.len == 0 || nd.len > 65535 || !nd.bytes) return fail(c, MK_ERR_BAD_ARG, "bad DFA table");
             size_t bytes = (size_t)nd.len * 65 * 2;
             h.bytes.assign(nd.bytes, nd.bytes + bytes);
             // every transition must name a state of the table
-            for (size_t s = 0; s < nd.len; s++)
+            for (size_t st = 0; st < nd.len; st++)
                 for (int v = 0; v < 64; v++) {
-                    uint32_t t = h.bytes[(s * 65 + v) * 2] | (uint32_t)h.bytes[(s * 65 + v) * 2 + 1] << 8;
-                    if (t >= nd.len) return bail(MK_ERR_BAD_ARG, "DFA transition out of range");
+                    uint32_t t = h.bytes[(st * 65 + v) * 2] | (uint32_t)h.bytes[(st * 65 + v) * 2 + 1] << 8;
+                    if (t >= nd.len) return fail(c, MK_ERR_BAD_ARG, "DFA transition out of range");
                 }
-            if (ms->n_regex >= 16) return bail(MK_ERR_BAD_ARG, "at most 16 regex needles per job");
-            uint8_t* d = nullptr;
-            if (cudaMalloc(&d, bytes) != cudaSuccess) return bail(MK_ERR_OUT_OF_MEMORY, "DFA allocation");
-            j->d_dfa.push_back(d);
-            if (cudaMemcpy(d, h.bytes.data(), bytes, cudaMemcpyHostToDevice) != cudaSuccess)
-                return bail(MK_ERR_CUDA, "DFA copy");
-            j->h2d += bytes;
-            ms->dfa[ms->n_regex] = d;
-            ms->dfa_states[ms->n_regex] = nd.len;
-            ms->regex_id[ms->n_regex] = (uint16_t)i;
-            ms->n_regex++;
+            if (ms.n_regex >= 16) return fail(c, MK_ERR_BAD_ARG, "at most 16 regex needles per job");
+            ms.dfa_states[ms.n_regex] = nd.len;
+            ms.regex_id[ms.n_regex] = (uint16_t)i;
+            ms.n_regex++;
         } else if (nd.mode == MK_MODE_CONTAINS || nd.mode == MK_MODE_SUFFIX) {
-            if (nd.len == 0 || nd.len > 43 || !nd.bytes) return bail(MK_ERR_BAD_ARG, "needle length must be 1..43");
+            if (nd.len == 0 || nd.len > 43 || !nd.bytes) return fail(c, MK_ERR_BAD_ARG, "needle length must be 1..43");
             h.bytes.assign(nd.bytes, nd.bytes + nd.len);
             for (auto& ch : h.bytes) {
-                if (b64_value(ch) < 0) return bail(MK_ERR_PATTERN, "needle character outside the base64 alphabet");
+                if (b64_value(ch) < 0) return fail(c, MK_ERR_PATTERN, "needle character outside the base64 alphabet");
                 if (h.fold && ch >= 'A' && ch <= 'Z') ch = (uint8_t)(ch + 32);
             }
-            // do not straddle a 64-bit word
             if ((bit & 63) + nd.len > 64) bit = (bit + 63) & ~63u;
-            if (bit + nd.len > 64u * mkb::SA_WORDS) return bail(MK_ERR_BAD_ARG, "needles exceed the shift-and state");
+            if (bit + nd.len > 64u * mkb::SA_WORDS) return fail(c, MK_ERR_BAD_ARG, "needles exceed the shift-and state");
             for (uint32_t k = 0; k < nd.len; k++) {
                 uint32_t b = bit + k;
                 uint8_t ch = h.bytes[k];
                 int v = b64_value(ch);
-                ms->mask[v][b >> 6] |= 1ull << (b & 63);
-                if (h.fold && ch >= 'a' && ch <= 'z') ms->mask[v - 26][b >> 6] |= 1ull << (b & 63);
+                ms.mask[v][b >> 6] |= 1ull << (b & 63);
+                if (h.fold && ch >= 'a' && ch <= 'z') ms.mask[v - 26][b >> 6] |= 1ull << (b & 63);
             }
-            ms->first_bit[bit >> 6] |= 1ull << (bit & 63);
+            ms.first_bit[bit >> 6] |= 1ull << (bit & 63);
             uint32_t last = bit + nd.len - 1;
-            if (nd.mode == MK_MODE_SUFFIX) ms->suffix_bit[last >> 6] |= 1ull << (last & 63);
-            else ms->last_bit[last >> 6] |= 1ull << (last & 63);
-            ms->text_id[ms->n_text] = (uint16_t)i;
-            ms->text_last[ms->n_text] = (uint16_t)last;
-            ms->n_text++;
+            if (nd.mode == MK_MODE_SUFFIX) ms.suffix_bit[last >> 6] |= 1ull << (last & 63);
+            else ms.last_bit[last >> 6] |= 1ull << (last & 63);
+            ms.text_id[ms.n_text] = (uint16_t)i;
+            ms.text_last[ms.n_text] = (uint16_t)last;
+            ms.n_text++;
             bit += nd.len;
         } else {
-            return bail(MK_ERR_BAD_ARG, "unknown needle mode");
+            return fail(c, MK_ERR_BAD_ARG, "unknown needle mode");
         }
-        j->needles.push_back(std::move(h));
+        hosts.push_back(std::move(h));
     }
-    ms->sa_words = ms->n_text ? (bit + 63) / 64 : 0;
-    if (cudaMalloc(&j->d_match, sizeof *ms) != cudaSuccess) return bail(MK_ERR_OUT_OF_MEMORY, "match allocation");
-    if (cudaMemcpy(j->d_match, ms, sizeof *ms, cudaMemcpyHostToDevice) != cudaSuccess) return bail(MK_ERR_CUDA, "match copy");
-    j->h2d += sizeof *ms;
-    delete ms;
-    ms = nullptr;
-    auto bail2 = [&](int code, const std::string& msg) {
+    ms.sa_words = ms.n_text ? (bit + 63) / 64 : 0;
+    return MK_OK;
+}
+
+// Uploads a packed MatchSet and its DFA tables to the job's device copy (after the job's
+// previous launches have finished).  DFA tables get fresh device buffers; text needles
+// need no allocation.
+static int upload_needles(mk_job* j, mkb::MatchSet& ms, std::vector<mkh25519::Needle>& hosts) {
+    mk_ctx* c = j->ctx;
+    MK_CUDA(c, cudaStreamSynchronize(c->stream));
+    for (auto d : j->d_dfa) cudaFree(d);
+    j->d_dfa.clear();
+    for (uint32_t r = 0; r < ms.n_regex; r++) {
+        const mkh25519::Needle& h = hosts[ms.regex_id[r]];
+        uint8_t* d = nullptr;
+        if (cudaMalloc(&d, h.bytes.size()) != cudaSuccess) return fail(c, MK_ERR_OUT_OF_MEMORY, "DFA allocation");
+        j->d_dfa.push_back(d);
+        MK_CUDA(c, cudaMemcpy(d, h.bytes.data(), h.bytes.size(), cudaMemcpyHostToDevice));
+        j->h2d += h.bytes.size();
+        ms.dfa[r] = d;
+    }
+    if (!j->d_match && cudaMalloc(&j->d_match, sizeof ms) != cudaSuccess) {
+        j->d_match = nullptr;
+        return fail(c, MK_ERR_OUT_OF_MEMORY, "match allocation");
+    }
+    MK_CUDA(c, cudaMemcpy(j->d_match, &ms, sizeof ms, cudaMemcpyHostToDevice));
+    j->h2d += sizeof ms;
+    j->needles = std::move(hosts);
+    return MK_OK;
+}
+
+int mk_job_prepare(mk_ctx* c, const uint8_t key[32], int seed_source, const mk_needle* needles, uint32_t n_needles,
+                   int stop_on_hit, mk_job** out) {
+    if (!c || !key || !out || (n_needles && !needles)) return fail(c, MK_ERR_BAD_ARG, "bad argument");
+    if (int st = check_source(c, key, seed_source)) return st;
+    *out = nullptr;
+    MK_CUDA(c, cudaSetDevice(c->device));
+    std::unique_ptr<mkb::MatchSet> ms(new (std::nothrow) mkb::MatchSet);
+    if (!ms) return fail(c, MK_ERR_OUT_OF_MEMORY, "host allocation");
+    std::vector<mkh25519::Needle> hosts;
+    if (int st = pack_needles(c, needles, n_needles, *ms, hosts)) return st;
+    mk_job* j = new (std::nothrow) mk_job;
+    if (!j) return fail(c, MK_ERR_OUT_OF_MEMORY, "host allocation");
+    j->ctx = c;
+    memcpy(j->key, key, 32);
+    j->source = seed_source;
+    j->stop_on_hit = stop_on_hit;
+    j->cap = c->hit_capacity;
+    auto bail = [&](int code, const std::string& msg) {
         mk_job_destroy(j);
         return fail(c, code, msg);
     };
-    if (cudaMalloc(&j->d_hits, sizeof(mkb::HitRecord) * j->cap) != cudaSuccess) return bail2(MK_ERR_OUT_OF_MEMORY, "hit ring");
-    if (cudaMalloc(&j->d_job, sizeof(mkb::JobDevice)) != cudaSuccess) return bail2(MK_ERR_OUT_OF_MEMORY, "job state");
-    if (cudaMemset(j->d_job, 0, sizeof(mkb::JobDevice)) != cudaSuccess) return bail2(MK_ERR_CUDA, "job state");
+    if (int st = upload_needles(j, *ms, hosts)) {
+        std::string keep = c->err;
+        mk_job_destroy(j);
+        return fail(c, st, keep);
+    }
+    if (cudaMalloc(&j->d_hits, sizeof(mkb::HitRecord) * j->cap) != cudaSuccess) return bail(MK_ERR_OUT_OF_MEMORY, "hit ring");
+    if (cudaMalloc(&j->d_job, sizeof(mkb::JobDevice)) != cudaSuccess) return bail(MK_ERR_OUT_OF_MEMORY, "job state");
+    if (cudaMemset(j->d_job, 0, sizeof(mkb::JobDevice)) != cudaSuccess) return bail(MK_ERR_CUDA, "job state");
     if (cudaMalloc(&j->d_sink, sizeof(uint32_t) * (size_t)c->grid * c->block) != cudaSuccess)
-        return bail2(MK_ERR_OUT_OF_MEMORY, "sink");
+        return bail(MK_ERR_OUT_OF_MEMORY, "sink");
     *out = j;
     return MK_OK;
+}
+
+int mk_job_update(mk_job* j, const mk_needle* needles, uint32_t n_needles) {
+    if (!j) return MK_ERR_BAD_ARG;
+    mk_ctx* c = j->ctx;
+    MK_CUDA(c, cudaSetDevice(c->device));
+    std::unique_ptr<mkb::MatchSet> ms(new (std::nothrow) mkb::MatchSet);
+    if (!ms) return fail(c, MK_ERR_OUT_OF_MEMORY, "host allocation");
+    std::vector<mkh25519::Needle> hosts;
+    if (int st = pack_needles(c, needles, n_needles, *ms, hosts)) return st;
+    return upload_needles(j, *ms, hosts);
 }
 
 void mk_job_destroy(mk_job* j) {
@@ -424,10 +524,9 @@ void mk_job_destroy(mk_job* j) {
     delete j;
 }
 
-static int enqueue(mk_job* j, uint64_t base, uint32_t iters) {
-    mk_ctx* c = j->ctx;
-    MK_CUDA(c, cudaSetDevice(c->device));
-    MK_CUDA(c, cudaMemsetAsync(j->d_job, 0, 8, c->stream));  // hit_count and status; keep stop
+// Kernel parameters of one search launch of a job.
+static mkb::KeyLaunch search_params(const mk_job* j, uint64_t base, uint32_t iters) {
+    const mk_ctx* c = j->ctx;
     mkb::KeyLaunch L{};
     L.table = c->table;
     L.geom = c->geom;
@@ -442,6 +541,15 @@ static int enqueue(mk_job* j, uint64_t base, uint32_t iters) {
     L.stop_on_hit = (uint32_t)j->stop_on_hit;
     L.job = j->d_job;
     L.sink = j->d_sink;
+    if (j->source == MK_SEED_INCREMENTAL) set_incremental(c, j->key, base, L);
+    return L;
+}
+
+static int enqueue(mk_job* j, uint64_t base, uint32_t iters) {
+    mk_ctx* c = j->ctx;
+    MK_CUDA(c, cudaSetDevice(c->device));
+    MK_CUDA(c, cudaMemsetAsync(j->d_job, 0, 8, c->stream));  // hit_count and status; keep stop
+    mkb::KeyLaunch L = search_params(j, base, iters);
     MK_CUDA(c, mkb::launch_keys(L, false, c->kpt, c->block, c->grid, c->stream));
     j->h2d += sizeof L;  // kernel parameters
     return MK_OK;
@@ -453,15 +561,9 @@ int mk_job_enqueue(mk_job* j, uint64_t base, uint32_t iters) {
     return enqueue(j, base, iters);
 }
 
-int mk_job_launch(mk_job* j, uint64_t base, uint32_t iters, int* found, uint64_t* index) {
-    if (!j) return MK_ERR_BAD_ARG;
+// Waits for the job's queued work, then reads its state and hit ring (sorted by index).
+static int collect(mk_job* j, int* found, uint64_t* index) {
     mk_ctx* c = j->ctx;
-    j->last.clear();
-    j->last_total = 0;
-    if (found) *found = 0;
-    if (iters == 0) return MK_OK;
-    int st = enqueue(j, base, iters);
-    if (st) return st;
     mkb::JobDevice jd;
     MK_CUDA(c, cudaMemcpyAsync(&jd, j->d_job, sizeof jd, cudaMemcpyDeviceToHost, c->stream));
     MK_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -484,6 +586,17 @@ int mk_job_launch(mk_job* j, uint64_t base, uint32_t iters, int* found, uint64_t
     return MK_OK;
 }
 
+int mk_job_launch(mk_job* j, uint64_t base, uint32_t iters, int* found, uint64_t* index) {
+    if (!j) return MK_ERR_BAD_ARG;
+    j->last.clear();
+    j->last_total = 0;
+    if (found) *found = 0;
+    if (iters == 0) return MK_OK;
+    int st = enqueue(j, base, iters);
+    if (st) return st;
+    return collect(j, found, index);
+}
+
 int mk_job_hits(mk_job* j, mk_hit* out, uint32_t cap, uint32_t* written, uint64_t* total) {
     if (!j || !written || !total || (cap && !out)) return MK_ERR_BAD_ARG;
     *total = j->last_total;
@@ -493,6 +606,22 @@ int mk_job_hits(mk_job* j, mk_hit* out, uint32_t cap, uint32_t* written, uint64_
     return j->last_total > j->cap ? MK_ERR_HIT_RING_FULL : MK_OK;
 }
 
+int mk_job_confirm(mk_job* j, uint64_t index, uint32_t needle, uint8_t pk[32], uint8_t secret[32], int* matched) {
+    if (!j || !pk || !secret || !matched) return MK_ERR_BAD_ARG;
+    if (needle >= j->needles.size()) return fail(j->ctx, MK_ERR_BAD_ARG, "needle index out of range");
+    *matched = 0;
+    if (j->source == MK_SEED_INCREMENTAL) {
+        if (!mkh25519::incremental_scalar(j->key, index, secret))
+            return fail(j->ctx, MK_ERR_BAD_ARG, "incremental start scalar must be below 2^255");
+        mkh25519::scalar_public_key(secret, pk);
+    } else {
+        mkh25519::seed_of(j->key, j->source, index, secret);
+        mkh25519::public_key(secret, pk);
+    }
+    *matched = mkh25519::matches(j->needles[needle], pk) ? 1 : 0;
+    return MK_OK;
+}
+
 int mk_job_io_bytes(const mk_job* j, uint64_t* h2d, uint64_t* d2h) {
     if (!j || !h2d || !d2h) return MK_ERR_BAD_ARG;
     *h2d = j->h2d;
@@ -500,8 +629,9 @@ int mk_job_io_bytes(const mk_job* j, uint64_t* h2d, uint64_t* d2h) {
     return MK_OK;
 }
 
-int mk_ctx_work_per_key(const mk_ctx* c, double* field_muls, double* int_mads) {
-    if (!c || !field_muls || !int_mads) return MK_ERR_BAD_ARG;
+int mk_ctx_work_per_key(const mk_ctx* c, int seed_source, double* field_muls, double* int_mads) {
+    if (!c || !field_muls || !int_mads || seed_source < MK_SEED_CHACHA20 || seed_source > MK_SEED_INCREMENTAL)
+        return MK_ERR_BAD_ARG;
     // radix-2^32 costs: a multiplication is 64 mad.lo + 64 mad.hi (8x8 limbs) + 16 (fold by 38),
     // a squaring 28 cross products + 8 diagonal ones (72) + 16
     const double MUL = 144.0, SQ = 88.0;
@@ -512,6 +642,12 @@ int mk_ctx_work_per_key(const mk_ctx* c, double* field_muls, double* int_mads) {
     // Montgomery batch inside a thread: a_j and the running product (2 each for j > 0),
     // back-sweep y_j = a_j·inv and inv·den_j
     double batch = (4.0 * (kpt - 1) + 1.0) / kpt;
+    if (seed_source == MK_SEED_INCREMENTAL) {
+        // no comb: key j > 0 of a thread's run is the y of Q + j·B (3 multiplications), and Q
+        // advances once per run by a full mixed addition (7); the thread's start point
+        // (at most 8 additions per launch) is left out
+        comb = (3.0 * (kpt - 1) + 7.0) / kpt;
+    }
     // pooled inversion by the CTA's inverter warp: each lane a pool of `groups` thread
     // products, 3(groups-1) multiplications and one inversion (254 squarings + 11 multiplications)
     double pool_mul = 32.0 * (3.0 * (groups - 1) + 11.0) / (ct * kpt);
@@ -521,11 +657,114 @@ int mk_ctx_work_per_key(const mk_ctx* c, double* field_muls, double* int_mads) {
     return MK_OK;
 }
 
-int mk_measure_imad_peak(mk_ctx* c, double* mads_per_s) {
-    if (!c || !mads_per_s) return MK_ERR_BAD_ARG;
+int mk_measure_mad_peaks(mk_ctx* c, double* chain_per_s, double* lo_per_s) {
+    if (!c || !chain_per_s || !lo_per_s) return MK_ERR_BAD_ARG;
     MK_CUDA(c, cudaSetDevice(c->device));
-    MK_CUDA(c, mkb::measure_imad((int)c->info.sms, c->stream, mads_per_s));
+    MK_CUDA(c, mkb::measure_mad_peaks((int)c->info.sms, c->stream, chain_per_s, lo_per_s));
     return MK_OK;
+}
+
+// ---- CUDA graph of a job's launches ----
+
+int mk_job_graph_create(mk_job* j, uint32_t iters, uint32_t launches, mk_graph** out) {
+    if (!j || !out || iters == 0 || launches == 0 || launches > 4096) return MK_ERR_BAD_ARG;
+    *out = nullptr;
+    mk_ctx* c = j->ctx;
+    MK_CUDA(c, cudaSetDevice(c->device));
+    mk_graph* g = new (std::nothrow) mk_graph;
+    if (!g) return fail(c, MK_ERR_OUT_OF_MEMORY, "host allocation");
+    g->job = j;
+    g->iters = iters;
+    g->span = c->info.keys_per_iter * iters;
+    g->params.resize(launches);
+    g->nodes.resize(launches);
+    auto bail = [&](cudaError_t e, const char* what) {
+        mk_graph_destroy(g);
+        return cuda_fail(c, e, what);
+    };
+    cudaError_t e = cudaGraphCreate(&g->graph, 0);
+    if (e != cudaSuccess) return bail(e, "cudaGraphCreate");
+    // reset hit count and status once; hits of all launches accumulate in the ring
+    cudaMemsetParams ms{};
+    ms.dst = j->d_job;
+    ms.value = 0;
+    ms.elementSize = 4;
+    ms.width = 2;
+    ms.height = 1;
+    ms.pitch = 0;
+    cudaGraphNode_t prev = nullptr;
+    e = cudaGraphAddMemsetNode(&prev, g->graph, nullptr, 0, &ms);
+    if (e != cudaSuccess) return bail(e, "cudaGraphAddMemsetNode");
+    const void* func = nullptr;
+    size_t dyn = 0;
+    e = mkb::keys_kernel(false, j->source == MK_SEED_INCREMENTAL, c->kpt, c->block, &func, &dyn);
+    if (e != cudaSuccess) return bail(e, "keys_kernel");
+    for (uint32_t i = 0; i < launches; i++) {
+        g->params[i] = search_params(j, g->span * i, iters);
+        void* args[] = {&g->params[i]};
+        cudaKernelNodeParams kp{};
+        kp.func = const_cast<void*>(func);
+        kp.gridDim = dim3(c->grid);
+        kp.blockDim = dim3(c->block);
+        kp.sharedMemBytes = (unsigned)dyn;
+        kp.kernelParams = args;
+        e = cudaGraphAddKernelNode(&g->nodes[i], g->graph, &prev, 1, &kp);
+        if (e != cudaSuccess) return bail(e, "cudaGraphAddKernelNode");
+        prev = g->nodes[i];
+    }
+    g->func = func;
+    g->dyn = dyn;
+    e = cudaGraphInstantiate(&g->exec, g->graph, 0);
+    if (e != cudaSuccess) return bail(e, "cudaGraphInstantiate");
+    *out = g;
+    return MK_OK;
+}
+
+// Points every kernel node at its range of base .. base + launches·span and enqueues the graph.
+static int graph_enqueue(mk_graph* g, uint64_t base) {
+    mk_job* j = g->job;
+    mk_ctx* c = j->ctx;
+    MK_CUDA(c, cudaSetDevice(c->device));
+    for (size_t i = 0; i < g->nodes.size(); i++) {
+        g->params[i] = search_params(j, base + g->span * i, g->iters);
+        void* args[] = {&g->params[i]};
+        cudaKernelNodeParams kp{};
+        kp.func = const_cast<void*>(g->func);
+        kp.gridDim = dim3(c->grid);
+        kp.blockDim = dim3(c->block);
+        kp.sharedMemBytes = (unsigned)g->dyn;
+        kp.kernelParams = args;
+        MK_CUDA(c, cudaGraphExecKernelNodeSetParams(g->exec, g->nodes[i], &kp));
+        j->h2d += sizeof(mkb::KeyLaunch);
+    }
+    MK_CUDA(c, cudaGraphLaunch(g->exec, c->stream));
+    return MK_OK;
+}
+
+int mk_graph_enqueue(mk_graph* g, uint64_t base) {
+    if (!g) return MK_ERR_BAD_ARG;
+    return graph_enqueue(g, base);
+}
+
+int mk_graph_launch(mk_graph* g, uint64_t base, int* found, uint64_t* index) {
+    if (!g) return MK_ERR_BAD_ARG;
+    mk_job* j = g->job;
+    j->last.clear();
+    j->last_total = 0;
+    if (found) *found = 0;
+    if (int st = graph_enqueue(g, base)) return st;
+    return collect(j, found, index);
+}
+
+void mk_graph_destroy(mk_graph* g) {
+    if (!g) return;
+    if (g->job && g->job->ctx) {
+        cudaSetDevice(g->job->ctx->device);
+        cudaStreamSynchronize(g->job->ctx->stream);
+    }
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    delete g;
 }
 
 int mk_ctx_sync(mk_ctx* c) {

@@ -317,6 +317,37 @@ void public_key(const uint8_t seed[32], uint8_t pk[32]) {
     compress(base_mul(h), pk);
 }
 
+void scalar_public_key(const uint8_t s[32], uint8_t pk[32]) { compress(base_mul(s), pk); }
+
+bool incremental_scalar(const uint8_t s0[32], uint64_t k, uint8_t s[32]) {
+    if (s0[31] & 0x80) return false;
+    u64 c = 0;
+    for (int b = 0; b < 32; b++) {
+        c += (u64)s0[b] + (b < 8 ? (k >> (8 * b)) & 0xff : 0);
+        s[b] = (uint8_t)c;
+        c >>= 8;
+    }
+    return true;
+}
+
+void scalar_point_words(const uint8_t s[32], uint32_t out[32]) {
+    Pt a = affine(base_mul(s));
+    to_words(a.X, out);
+    to_words(a.Y, out + 8);
+    to_words(a.Z, out + 16);
+    to_words(a.T, out + 24);
+}
+
+void niels_of_multiple(uint64_t k, uint32_t out[24]) {
+    const Consts& C = consts();
+    uint8_t s[32] = {};
+    for (int b = 0; b < 8; b++) s[b] = (uint8_t)(k >> (8 * b));
+    Pt a = affine(base_mul(s));
+    to_words(a.Y + a.X, out);
+    to_words(a.Y - a.X, out + 8);
+    to_words(a.T * C.d2, out + 16);
+}
+
 void public_b64(const uint8_t pk[32], char out[68]) {
     static const char HEAD[] = "AAAAC3NzaC1lZDI1NTE5AAAA";
     memcpy(out, HEAD, 24);

@@ -22,6 +22,17 @@ void sha512(const uint8_t* msg, size_t len, uint8_t out[64]);
 // compressed public key of a 32-byte seed (RFC 8032 5.1.5)
 void public_key(const uint8_t seed[32], uint8_t pk[32]);
 
+// Incremental (low-security) path: index k stands for the scalar s0 + k itself (no hashing,
+// no clamping), so its public key is (s0 + k)·B.  s0 must be below 2^255 (false otherwise),
+// which keeps s0 + k below 2^256 for every 64-bit k.
+bool incremental_scalar(const uint8_t s0[32], uint64_t k, uint8_t s[32]);
+// compressed public key of the 256-bit little-endian scalar s
+void scalar_public_key(const uint8_t s[32], uint8_t pk[32]);
+// s·B as extended coordinates with Z = 1: x, y, 1, xy (8 canonical LE words each)
+void scalar_point_words(const uint8_t s[32], uint32_t out[32]);
+// k·B in the table form (y+x, y-x, 2d·xy), 8 canonical LE words each; k = 0 gives (1, 1, 0)
+void niels_of_multiple(uint64_t k, uint32_t out[24]);
+
 // 68 base64 characters of the OpenSSH key blob (no terminator)
 void public_b64(const uint8_t pk[32], char out[68]);
 

@@ -398,6 +398,79 @@ __device__ __forceinline__ void invert_pools(fe* prod, fe* scratch, int groups) 
     prod[l] = inv;
 }
 
+// ---------------------------------------------------------------------------
+// incremental source: index base + i is the point (s0 + base + i)·B
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ fe words_fe(const u32* w) {
+    fe r;
+#pragma unroll
+    for (int i = 0; i < 8; i++) r.v[i] = w[i];
+    return r;
+}
+
+__device__ __forceinline__ niels words_niels(const u32* w) {
+    niels n;
+    n.ypx = words_fe(w);
+    n.ymx = words_fe(w + 8);
+    n.t2d = words_fe(w + 16);
+    return n;
+}
+
+__device__ __forceinline__ niels smem_niels(const uint4* q) {
+    niels n;
+    uint4 a;
+    a = q[0]; n.ypx.v[0] = a.x; n.ypx.v[1] = a.y; n.ypx.v[2] = a.z; n.ypx.v[3] = a.w;
+    a = q[1]; n.ypx.v[4] = a.x; n.ypx.v[5] = a.y; n.ypx.v[6] = a.z; n.ypx.v[7] = a.w;
+    a = q[2]; n.ymx.v[0] = a.x; n.ymx.v[1] = a.y; n.ymx.v[2] = a.z; n.ymx.v[3] = a.w;
+    a = q[3]; n.ymx.v[4] = a.x; n.ymx.v[5] = a.y; n.ymx.v[6] = a.z; n.ymx.v[7] = a.w;
+    a = q[4]; n.t2d.v[0] = a.x; n.t2d.v[1] = a.y; n.t2d.v[2] = a.z; n.t2d.v[3] = a.w;
+    a = q[5]; n.t2d.v[4] = a.x; n.t2d.v[5] = a.y; n.t2d.v[6] = a.z; n.t2d.v[7] = a.w;
+    return n;
+}
+
+// The launch's start point (s0 + base)·B plus offset·B from the 4-bit window table
+// (offset < 2^32; one mixed addition per nonzero window).
+__device__ __forceinline__ ge incr_start(const KeyLaunch& L, u64 offset) {
+    ge P;
+    P.X = words_fe(L.start);
+    P.Y = words_fe(L.start + 8);
+    P.Z = words_fe(L.start + 16);
+    P.T = words_fe(L.start + 24);
+#pragma unroll 1
+    for (int w = 0; w < INCR_WINDOWS; w++) {
+        const u32 d = (u32)(offset >> (4 * w)) & 15u;
+        if (d) P = mk32::ge_add_niels(P, load_entry(L.incr, (u64)w * 16 + d), false);
+    }
+    return P;
+}
+
+// Copies the step table j·B (j = 0 .. INCR_STEPS-1) into shared memory.
+__device__ __forceinline__ void load_steps(const KeyLaunch& L, uint4* steps, u32 tid, u32 nthr) {
+    const uint4* src = L.incr + (u64)INCR_WINDOWS * 16 * (ENTRY_WORDS / 4);
+    for (u32 i = tid; i < (u32)INCR_STEPS * (ENTRY_WORDS / 4); i += nthr) steps[i] = src[i];
+}
+
+// Batch of the KPT consecutive points Q + j·B (j = 0 .. KPT-1): key 0 is Q itself (y = Y/Z);
+// key j > 0 takes y = (b + a)/(2Z - c) of the mixed addition with the step entry j·B,
+// three multiplications, with Q's y+x, y-x and 2Z shared by all of them.
+template <int KPT>
+__device__ __forceinline__ void incr_fracs(const ge& Q, const uint4* steps, Batch<KPT>& b) {
+    const fe ypx = mk32::fe_add(Q.Y, Q.X), ymx = mk32::fe_sub(Q.Y, Q.X), z2 = mk32::fe_add(Q.Z, Q.Z);
+    b.a[0] = Q.Y;
+    b.den[0] = Q.Z;
+    fe run = Q.Z;
+#pragma unroll 1
+    for (int j = 1; j < KPT; j++) {
+        const niels t = smem_niels(steps + j * (ENTRY_WORDS / 4));
+        const fe A = mk32::fe_mul(ymx, t.ymx), B = mk32::fe_mul(ypx, t.ypx), C = mk32::fe_mul(Q.T, t.t2d);
+        b.den[j] = mk32::fe_sub(z2, C);
+        b.a[j] = mk32::fe_mul(mk32::fe_add(B, A), run);
+        run = mk32::fe_mul(run, b.den[j]);
+    }
+    b.prod = run;
+}
+
 // Search kernel.  The CTA's last warp only inverts; the other BLOCK-32 threads each handle
 // KPT consecutive indices per iteration (index = base + (it·nthreads + gid)·KPT + j, where
 // gid and nthreads count these compute threads).  Iterations are pipelined two deep: a
@@ -407,7 +480,10 @@ __device__ __forceinline__ void invert_pools(fe* prod, fe* scratch, int groups) 
 // waits; inverses of buffer b ready (3 + b): the inverter arrives, compute warps wait.
 // Stop requests (host stop word, or a hit with stop_on_hit) are read by the inverter and
 // take effect two iterations later, at a point every warp agrees on.
-template <int KPT, int BLOCK>
+// INCR: the incremental source.  A compute thread keeps the point Q of its first index in
+// the current iteration; its keys are Q + j·B from the step table, and Q advances by
+// keys_per_iter·B (one mixed addition) per iteration.  No comb table is read.
+template <int KPT, int BLOCK, bool INCR>
 __global__ void __launch_bounds__(BLOCK, 512 / BLOCK) k_search(const KeyLaunch L) {
     constexpr int CT = BLOCK - 32;      // compute threads
     constexpr int CW = CT / 32;         // compute warps = pool length per inverter lane
@@ -420,7 +496,9 @@ __global__ void __launch_bounds__(BLOCK, 512 / BLOCK) k_search(const KeyLaunch L
     __shared__ u32 key[8];
     __shared__ mkh::CounterMid mid;
     __shared__ volatile u32 stop_iter;
+    __shared__ uint4 steps[INCR ? INCR_STEPS * (ENTRY_WORDS / 4) : 1];
     const u32 tid = threadIdx.x;
+    if (INCR) load_steps(L, steps, tid, BLOCK);
     {
         const u32* src = (const u32*)&L.geom;
         u32* dst = (u32*)&g;
@@ -462,15 +540,22 @@ __global__ void __launch_bounds__(BLOCK, 512 / BLOCK) k_search(const KeyLaunch L
     // ---- compute warps ----
     const u64 gid = (u64)blockIdx.x * CT + tid;
     const u64 nthreads = (u64)gridDim.x * CT;
-    EntrySlot& slot = slots[tid];
+    EntrySlot& slot = slots[INCR ? 0 : tid];
     Batch<KPT> batch[2];
     u64 sc[KPT][4];
     u32 sink = 0;
+    ge Q;
+    if (INCR) Q = incr_start(L, gid * KPT);
     auto first_of = [&](u32 it) { return L.base + ((u64)it * nthreads + gid) * KPT; };
     auto produce = [&](u32 it) {
         const int b = it & 1;
-        scalars<KPT>(L, key, mid, first_of(it), sc);
-        combs<KPT>(L, g, sc, slot, batch[b]);
+        if (INCR) {
+            incr_fracs<KPT>(Q, steps, batch[b]);
+            Q = mk32::ge_add_niels(Q, words_niels(L.delta), false);
+        } else {
+            scalars<KPT>(L, key, mid, first_of(it), sc);
+            combs<KPT>(L, g, sc, slot, batch[b]);
+        }
         prod[b][tid] = batch[b].prod;
         bar_arrive(1 + b, BLOCK);
     };
@@ -486,8 +571,10 @@ __global__ void __launch_bounds__(BLOCK, 512 / BLOCK) k_search(const KeyLaunch L
 }
 
 // Derive kernel: full public keys (x sign included) of indices base .. base+count-1;
-// one iteration, per-CTA pooled inversion of 2·KPT denominators per thread.
-template <int KPT, int BLOCK>
+// one iteration, per-CTA pooled inversion of 2·KPT denominators per thread.  INCR: the
+// thread's keys are Q + j·B with Q = (s0 + first)·B; key j gives y = (b+a)/(2Z-c) and
+// x = (b-a)/(2Z+c) of the mixed addition with step entry j (entry 0 is the identity).
+template <int KPT, int BLOCK, bool INCR>
 __global__ void __launch_bounds__(BLOCK, 512 / BLOCK) k_derive(const KeyLaunch L) {
     constexpr int NUM = 2 * KPT;
     extern __shared__ uint4 dyn_smem[];
@@ -496,8 +583,10 @@ __global__ void __launch_bounds__(BLOCK, 512 / BLOCK) k_derive(const KeyLaunch L
     EntrySlot* slots = reinterpret_cast<EntrySlot*>(scratch + BLOCK);
     __shared__ CombGeom g;
     __shared__ u32 key[8];
+    __shared__ uint4 steps[INCR ? INCR_STEPS * (ENTRY_WORDS / 4) : 1];
     const u32 tid = threadIdx.x;
     const u64 gid = (u64)blockIdx.x * BLOCK + tid;
+    if (INCR) load_steps(L, steps, tid, BLOCK);
     {
         const u32* src = (const u32*)&L.geom;
         u32* dst = (u32*)&g;
@@ -511,11 +600,28 @@ __global__ void __launch_bounds__(BLOCK, 512 / BLOCK) k_derive(const KeyLaunch L
     fe num[NUM], den[NUM], pre[NUM];
     u32 blk[16];
     u64 blk_id = ~0ull;
+    ge Q;
+    fe ypx, ymx, z2;
+    if (INCR) {
+        Q = incr_start(L, gid * KPT);
+        ypx = mk32::fe_add(Q.Y, Q.X);
+        ymx = mk32::fe_sub(Q.Y, Q.X);
+        z2 = mk32::fe_add(Q.Z, Q.Z);
+    }
 #pragma unroll 1
     for (int j = 0; j < KPT; j++) {
-        u64 s[4];
-        scalar_of(L.seed_src, key, mid, first + (u64)j, blk, blk_id, s);
-        comb_mul(L.table, g, s, slots[tid], num[2 * j], den[2 * j], &num[2 * j + 1], &den[2 * j + 1]);
+        if (INCR) {
+            const niels t = smem_niels(steps + j * (ENTRY_WORDS / 4));
+            const fe A = mk32::fe_mul(ymx, t.ymx), B = mk32::fe_mul(ypx, t.ypx), C = mk32::fe_mul(Q.T, t.t2d);
+            num[2 * j] = mk32::fe_add(B, A);
+            den[2 * j] = mk32::fe_sub(z2, C);
+            num[2 * j + 1] = mk32::fe_sub(B, A);
+            den[2 * j + 1] = mk32::fe_add(z2, C);
+        } else {
+            u64 s[4];
+            scalar_of(L.seed_src, key, mid, first + (u64)j, blk, blk_id, s);
+            comb_mul(L.table, g, s, slots[tid], num[2 * j], den[2 * j], &num[2 * j + 1], &den[2 * j + 1]);
+        }
         pre[2 * j] = j == 0 ? den[0] : mk32::fe_mul(pre[2 * j - 1], den[2 * j]);
         pre[2 * j + 1] = mk32::fe_mul(pre[2 * j], den[2 * j + 1]);
     }
@@ -552,15 +658,19 @@ __global__ void __launch_bounds__(BLOCK, 512 / BLOCK) k_derive(const KeyLaunch L
 
 // dynamic shared memory: products and inversion scratch (two buffers each for the
 // search pipeline) and the per-thread table staging slots
-static size_t dyn_bytes(bool derive, uint32_t block) {
+// (the incremental source reads no comb table and needs no staging slots)
+static size_t dyn_bytes(bool derive, bool incr, uint32_t block) {
     const size_t fe_bytes = 32;
     const size_t threads = derive ? block : block - 32;  // the search kernel's last warp only inverts
-    return (derive ? 2 : 4) * threads * fe_bytes + threads * sizeof(EntrySlot);
+    return (derive ? 2 : 4) * threads * fe_bytes + (incr ? 0 : threads * sizeof(EntrySlot));
 }
 
-static const void* kernel_of(bool derive, uint32_t kpt, uint32_t block) {
-#define MK_FN(K, B) \
-    if (kpt == K && block == B) return derive ? (const void*)k_derive<K, B> : (const void*)k_search<K, B>;
+static const void* kernel_of(bool derive, bool incr, uint32_t kpt, uint32_t block) {
+#define MK_FN(K, B)                                                                                        \
+    if (kpt == K && block == B) {                                                                          \
+        if (incr) return derive ? (const void*)k_derive<K, B, true> : (const void*)k_search<K, B, true>;   \
+        return derive ? (const void*)k_derive<K, B, false> : (const void*)k_search<K, B, false>;           \
+    }
     MK_VARIANTS(MK_FN)
 #undef MK_FN
     return nullptr;
@@ -571,19 +681,29 @@ static cudaError_t prepare(const void* f, size_t dyn) {
 }
 
 cudaError_t launch_keys(const KeyLaunch& L, bool derive, uint32_t kpt, uint32_t block, uint32_t grid, cudaStream_t st) {
-    const void* f = kernel_of(derive, kpt, block);
+    const bool incr = L.seed_src == SEED_INCREMENTAL;
+    if (incr && (kpt > (uint32_t)INCR_STEPS || !L.incr)) return cudaErrorInvalidValue;
+    const void* f = kernel_of(derive, incr, kpt, block);
     if (!f) return cudaErrorInvalidValue;
-    const size_t dyn = dyn_bytes(derive, block);
+    const size_t dyn = dyn_bytes(derive, incr, block);
     cudaError_t e = prepare(f, dyn);
     if (e != cudaSuccess) return e;
     void* args[] = {const_cast<KeyLaunch*>(&L)};
     return cudaLaunchKernel(f, dim3(grid), dim3(block), args, dyn, st);
 }
 
-cudaError_t keys_occupancy(bool derive, uint32_t kpt, uint32_t block, int* blocks_per_sm) {
-    const void* f = kernel_of(derive, kpt, block);
+cudaError_t keys_kernel(bool derive, bool incr, uint32_t kpt, uint32_t block, const void** func, size_t* dyn) {
+    const void* f = kernel_of(derive, incr, kpt, block);
     if (!f) return cudaErrorInvalidValue;
-    const size_t dyn = dyn_bytes(derive, block);
+    *func = f;
+    *dyn = dyn_bytes(derive, incr, block);
+    return prepare(f, *dyn);
+}
+
+cudaError_t keys_occupancy(bool derive, bool incr, uint32_t kpt, uint32_t block, int* blocks_per_sm) {
+    const void* f = kernel_of(derive, incr, kpt, block);
+    if (!f) return cudaErrorInvalidValue;
+    const size_t dyn = dyn_bytes(derive, incr, block);
     cudaError_t e = prepare(f, dyn);
     if (e != cudaSuccess) return e;
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, f, (int)block, dyn);
@@ -601,7 +721,7 @@ cudaError_t launch_build_table(uint4* table, const CombGeom& g, const uint32_t* 
 namespace mkb {
 
 // Peak of independent 32-bit multiply-adds: 8 chains per thread, no memory traffic.
-__global__ void __launch_bounds__(256) k_imad_peak(uint32_t iters, uint32_t x, uint32_t y, uint32_t* out) {
+__global__ void __launch_bounds__(256) k_mad_lo_peak(uint32_t iters, uint32_t x, uint32_t y, uint32_t* out) {
     uint32_t a[8];
 #pragma unroll
     for (int i = 0; i < 8; i++) a[i] = threadIdx.x + i;
@@ -615,31 +735,89 @@ __global__ void __launch_bounds__(256) k_imad_peak(uint32_t iters, uint32_t x, u
     out[(uint64_t)blockIdx.x * blockDim.x + threadIdx.x] = s;
 }
 
-cudaError_t measure_imad(int sms, cudaStream_t st, double* mads_per_s) {
-    const uint32_t blocks = (uint32_t)sms * 8, threads = 256, iters = 1u << 17;
+// Peak of the field multiply's own instruction shape: one row of a schoolbook product,
+// acc[0..8] += a·b[0..7] as a mad.lo.cc/madc.lo.cc chain followed by the madc.hi.cc chain
+// one word up (16 multiply-adds and one addc), on four independent accumulators per thread.
+// The multiplier a is the accumulator's top word plus the iteration, so no product can be
+// hoisted out of the loop.
+__global__ void __launch_bounds__(256) k_mad_chain_peak(uint32_t iters, uint32_t seed, uint32_t* out) {
+    uint32_t acc[4][9], b[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) b[i] = seed * (2 * i + 1) + threadIdx.x;
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+#pragma unroll
+        for (int i = 0; i < 9; i++) acc[q][i] = threadIdx.x ^ (q * 9 + i);
+    for (uint32_t it = 0; it < iters; it++) {
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            uint32_t* t = acc[q];
+            const uint32_t a = t[8] + it;
+            asm volatile(
+                "mad.lo.cc.u32 %0, %9, %10, %0;\n\t"
+                "madc.lo.cc.u32 %1, %9, %11, %1;\n\t"
+                "madc.lo.cc.u32 %2, %9, %12, %2;\n\t"
+                "madc.lo.cc.u32 %3, %9, %13, %3;\n\t"
+                "madc.lo.cc.u32 %4, %9, %14, %4;\n\t"
+                "madc.lo.cc.u32 %5, %9, %15, %5;\n\t"
+                "madc.lo.cc.u32 %6, %9, %16, %6;\n\t"
+                "madc.lo.cc.u32 %7, %9, %17, %7;\n\t"
+                "addc.u32 %8, %8, 0;\n\t"
+                "mad.hi.cc.u32 %1, %9, %10, %1;\n\t"
+                "madc.hi.cc.u32 %2, %9, %11, %2;\n\t"
+                "madc.hi.cc.u32 %3, %9, %12, %3;\n\t"
+                "madc.hi.cc.u32 %4, %9, %13, %4;\n\t"
+                "madc.hi.cc.u32 %5, %9, %14, %5;\n\t"
+                "madc.hi.cc.u32 %6, %9, %15, %6;\n\t"
+                "madc.hi.cc.u32 %7, %9, %16, %7;\n\t"
+                "madc.hi.u32 %8, %9, %17, %8;\n\t"
+                : "+r"(t[0]), "+r"(t[1]), "+r"(t[2]), "+r"(t[3]), "+r"(t[4]), "+r"(t[5]), "+r"(t[6]), "+r"(t[7]),
+                  "+r"(t[8])
+                : "r"(a), "r"(b[0]), "r"(b[1]), "r"(b[2]), "r"(b[3]), "r"(b[4]), "r"(b[5]), "r"(b[6]), "r"(b[7]));
+        }
+    }
+    uint32_t s = 0;
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+#pragma unroll
+        for (int i = 0; i < 9; i++) s ^= acc[q][i];
+    out[(uint64_t)blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+// Best of three timed runs (after a short warm-up) of both microbenchmarks, each about
+// 10-30 ms at full occupancy: multiply-adds per second.
+cudaError_t measure_mad_peaks(int sms, cudaStream_t st, double* chain_per_s, double* lo_per_s) {
+    const uint32_t blocks = (uint32_t)sms * 8, threads = 256;
     uint32_t* out = nullptr;
     cudaError_t e = cudaMalloc(&out, sizeof(uint32_t) * blocks * threads);
     if (e != cudaSuccess) return e;
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    double best = 0;
-    k_imad_peak<<<blocks, threads, 0, st>>>(iters / 16, 0x12345u, 0x9876u, out);  // warm-up
-    for (int rep = 0; rep < 3 && e == cudaSuccess; rep++) {
+    double best_chain = 0, best_lo = 0;
+    const uint32_t lo_iters = 1u << 17, chain_iters = 1u << 14;
+    k_mad_lo_peak<<<blocks, threads, 0, st>>>(lo_iters / 16, 0x12345u, 0x9876u, out);
+    k_mad_chain_peak<<<blocks, threads, 0, st>>>(chain_iters / 16, 0x2468u, out);
+    for (int rep = 0; rep < 6 && e == cudaSuccess; rep++) {
+        const bool chain = rep & 1;
         cudaEventRecord(e0, st);
-        k_imad_peak<<<blocks, threads, 0, st>>>(iters, 0x12345u + rep, 0x9876u, out);
+        if (chain) k_mad_chain_peak<<<blocks, threads, 0, st>>>(chain_iters, 0x2468u + rep, out);
+        else k_mad_lo_peak<<<blocks, threads, 0, st>>>(lo_iters, 0x12345u + rep, 0x9876u, out);
         cudaEventRecord(e1, st);
         e = cudaEventSynchronize(e1);
         if (e == cudaSuccess) e = cudaGetLastError();
         float ms = 0;
         if (e == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
-        double ops = (double)blocks * threads * iters * 8;
-        if (ms > 0 && ops / (ms * 1e-3) > best) best = ops / (ms * 1e-3);
+        if (ms <= 0) continue;
+        const double mads = (double)blocks * threads * (chain ? (double)chain_iters * 4 * 16 : (double)lo_iters * 8);
+        double& best = chain ? best_chain : best_lo;
+        if (mads / (ms * 1e-3) > best) best = mads / (ms * 1e-3);
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     cudaFree(out);
-    *mads_per_s = best;
+    *chain_per_s = best_chain;
+    *lo_per_s = best_lo;
     return e;
 }
 

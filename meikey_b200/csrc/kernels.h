@@ -11,7 +11,7 @@ struct KeyLaunch {
     const uint4* table;
     CombGeom geom;
     uint32_t key[8];
-    uint32_t seed_src;     // 0 ChaCha20, 1 counter
+    uint32_t seed_src;     // 0 ChaCha20, 1 counter, 2 incremental
     uint32_t iters;
     uint64_t base;
     // search
@@ -24,11 +24,24 @@ struct KeyLaunch {
     // derive
     uint8_t* out;
     uint64_t count;
+    // incremental source: index base + i stands for the point (s0 + base + i)·B
+    const uint4* incr;     // INCR_WINDOWS·16 entries j·16^w·B, then INCR_STEPS entries j·B (table form)
+    uint32_t start[32];    // (s0 + base)·B as x, y, 1, xy
+    uint32_t delta[24];    // keys_per_iter·B: one search thread's jump between iterations
 };
 
+constexpr uint32_t SEED_INCREMENTAL = 2;
+constexpr int INCR_WINDOWS = 8;   // 4-bit windows of a thread's offset (offsets below 2^32)
+constexpr int INCR_STEPS = 16;    // j·B for j = 0 .. keys per thread - 1
+constexpr int INCR_ENTRIES = INCR_WINDOWS * 16 + INCR_STEPS;
+
 cudaError_t launch_keys(const KeyLaunch& L, bool derive, uint32_t kpt, uint32_t block, uint32_t grid, cudaStream_t st);
-cudaError_t keys_occupancy(bool derive, uint32_t kpt, uint32_t block, int* blocks_per_sm);
-cudaError_t measure_imad(int sms, cudaStream_t st, double* mads_per_s);
+// The kernel of a variant and its dynamic shared memory (for graph nodes); sets the
+// kernel's shared-memory limit like launch_keys does.
+cudaError_t keys_kernel(bool derive, bool incr, uint32_t kpt, uint32_t block, const void** func, size_t* dyn);
+cudaError_t keys_occupancy(bool derive, bool incr, uint32_t kpt, uint32_t block, int* blocks_per_sm);
+// multiply-adds per second of the carry-chain row microbenchmark and of plain mad.lo.u32
+cudaError_t measure_mad_peaks(int sms, cudaStream_t st, double* chain_per_s, double* lo_per_s);
 
 // Largest n of mk_derive_noalloc and the device address of its fixed staging array on
 // `device` (looked up once per device; the device must be current).

@@ -106,17 +106,18 @@ class Context:
     def job(self, key: bytes, source: int, needles: Sequence[Needle], stop_on_hit: bool = False) -> "Job":
         return Job(self, key, source, needles, stop_on_hit)
 
-    def work_per_key(self):
-        """(field multiplications, 32-bit integer MADs) per key of the search kernel."""
+    def work_per_key(self, source: int = L.SEED_CHACHA20):
+        """(field multiplications, 32-bit integer MADs) per key of the search kernel for a seed source."""
         fm, im = ctypes.c_double(), ctypes.c_double()
-        _check(self._lib, self._ptr, self._lib.mk_ctx_work_per_key(self._ptr, ctypes.byref(fm), ctypes.byref(im)))
+        _check(self._lib, self._ptr, self._lib.mk_ctx_work_per_key(self._ptr, source, ctypes.byref(fm),
+                                                                   ctypes.byref(im)))
         return fm.value, im.value
 
-    def measure_imad_peak(self) -> float:
-        """Measured 32-bit integer MADs per second of the device (bounded microbenchmark)."""
-        v = ctypes.c_double()
-        _check(self._lib, self._ptr, self._lib.mk_measure_imad_peak(self._ptr, ctypes.byref(v)))
-        return v.value
+    def measure_mad_peaks(self):
+        """(carry-chain row MADs/s, plain mad.lo MADs/s) of the device (bounded microbenchmarks)."""
+        a, b = ctypes.c_double(), ctypes.c_double()
+        _check(self._lib, self._ptr, self._lib.mk_measure_mad_peaks(self._ptr, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
 
     def sync(self):
         _check(self._lib, self._ptr, self._lib.mk_ctx_sync(self._ptr))
@@ -147,6 +148,17 @@ class Context:
             pass
 
 
+def _needle_array(needles: Sequence[Needle]):
+    """(mk_needle array, buffers to keep alive) for a list of needles."""
+    arr = (L.NeedleC * max(1, len(needles)))()
+    keep = []
+    for i, n in enumerate(needles):
+        buf = (ctypes.c_uint8 * max(1, len(n.text))).from_buffer_copy(n.text if n.text else b"\0")
+        keep.append(buf)
+        arr[i] = L.NeedleC(ctypes.cast(buf, ctypes.POINTER(ctypes.c_uint8)), n.c_len(), int(n.fold), n.mode)
+    return arr, keep
+
+
 class Job:
     """Key + needles + hit ring on the device (the reference's ``Launch``)."""
 
@@ -156,12 +168,7 @@ class Job:
         self.ctx = ctx
         self._lib = ctx._lib
         self.needles = list(needles)
-        arr = (L.NeedleC * max(1, len(self.needles)))()
-        self._keep = []
-        for i, n in enumerate(self.needles):
-            buf = (ctypes.c_uint8 * max(1, len(n.text))).from_buffer_copy(n.text if n.text else b"\0")
-            self._keep.append(buf)
-            arr[i] = L.NeedleC(ctypes.cast(buf, ctypes.POINTER(ctypes.c_uint8)), n.c_len(), int(n.fold), n.mode)
+        arr, self._keep = _needle_array(self.needles)
         ptr = ctypes.c_void_p()
         _check(self._lib, ctx._ptr, self._lib.mk_job_prepare(ctx._ptr, bytes(key), source, arr, len(self.needles),
                                                              1 if stop_on_hit else 0, ctypes.byref(ptr)))
@@ -185,6 +192,26 @@ class Job:
             _check(self._lib, self.ctx._ptr, st)
         return [(int(out[i].index), int(out[i].needle)) for i in range(written.value)], int(total.value)
 
+    def update(self, needles: Sequence[Needle]):
+        """Replace the needles between launches (hits then carry positions in the new list)."""
+        self.needles = list(needles)
+        arr, self._keep = _needle_array(self.needles)
+        _check(self._lib, self.ctx._ptr, self._lib.mk_job_update(self._ptr, arr, len(self.needles)))
+
+    def graph(self, iters: int, launches: int) -> "Graph":
+        """A CUDA graph of `launches` launches of `iters` iterations each (mk_job_graph_create)."""
+        return Graph(self, iters, launches)
+
+    def confirm(self, index: int, needle: int):
+        """Host confirmation of a candidate: (matched, public key, secret).  The secret is the
+        seed (ChaCha20 / counter sources) or the scalar s0 + index (incremental source)."""
+        pk = ctypes.create_string_buffer(32)
+        secret = ctypes.create_string_buffer(32)
+        ok = ctypes.c_int()
+        _check(self._lib, self.ctx._ptr, self._lib.mk_job_confirm(self._ptr, index, needle, pk, secret,
+                                                                  ctypes.byref(ok)))
+        return bool(ok.value), pk.raw, secret.raw
+
     def io_bytes(self):
         """(host->device, device->host) bytes this job has copied so far."""
         a, b = ctypes.c_uint64(), ctypes.c_uint64()
@@ -197,6 +224,47 @@ class Job:
     def close(self):
         if self._ptr:
             self._lib.mk_job_destroy(self._ptr)
+            self._ptr = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Graph:
+    """A job's consecutive launches captured as one CUDA graph (mk_job_graph_create)."""
+
+    def __init__(self, job: Job, iters: int, launches: int):
+        self.job = job
+        self._lib = job._lib
+        self.span = job.ctx.keys_per_iter * iters * launches
+        ptr = ctypes.c_void_p()
+        _check(self._lib, job.ctx._ptr, self._lib.mk_job_graph_create(job._ptr, iters, launches, ctypes.byref(ptr)))
+        self._ptr = ptr
+
+    def launch(self, base: int) -> Optional[int]:
+        """Replays the graph over base .. base + span - 1; the lowest candidate index or None."""
+        found = ctypes.c_int()
+        idx = ctypes.c_uint64()
+        st = self._lib.mk_graph_launch(self._ptr, base, ctypes.byref(found), ctypes.byref(idx))
+        if st not in (L.OK, L.ERR_STOPPED):
+            _check(self._lib, self.job.ctx._ptr, st)
+        return int(idx.value) if found.value else None
+
+    def enqueue(self, base: int):
+        _check(self._lib, self.job.ctx._ptr, self._lib.mk_graph_enqueue(self._ptr, base))
+
+    def close(self):
+        if self._ptr:
+            self._lib.mk_graph_destroy(self._ptr)
             self._ptr = ctypes.c_void_p()
 
     def __enter__(self):

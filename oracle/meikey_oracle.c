@@ -411,30 +411,43 @@ EXPORT void mko_seed(const u8 key[32], u32 src, u64 index, u8 seed[32]) {
     else mko_chacha20_seed(key, index, seed);
 }
 
+/* incremental path: compressed (s0 + k)·B = s0·B + k·B for k = first .. first+n-1.
+ * s0 is a 256-bit little-endian scalar below 2^255 (the caller's contract), so s0 + k
+ * never wraps.  There is no reference kernel for this path: the definition is the
+ * point sequence P_k = P_0 + k·B of the incremental (low-security) configuration. */
+static void incremental_pubkey(const u8 s0[32], u64 k, u8 pk[32]) {
+    u8 s[32];
+    u64 c = 0;
+    for (int b = 0; b < 32; b++) {
+        u64 add = b < 8 ? (k >> (8 * b)) & 0xff : 0;
+        c += (u64)s0[b] + add;
+        s[b] = (u8)c;
+        c >>= 8;
+    }
+    ge_compress(base_mul(s), pk);
+}
+
+EXPORT void mko_incremental(const u8 s0[32], u64 first, u64 n, u8* out) {
+    oracle_init();
+    for (u64 i = 0; i < n; i++) incremental_pubkey(s0, first + i, out + 32 * i);
+}
+
+/* public key of one index of source src (0 ChaCha20, 1 counter: Ed25519 key of the seed;
+ * 2 incremental: (key + index)·B with key the start scalar) */
+static void index_pubkey(const u8 key[32], u32 src, u64 index, u8 pk[32]) {
+    if (src == 2) {
+        incremental_pubkey(key, index, pk);
+        return;
+    }
+    u8 seed[32];
+    mko_seed(key, src, index, seed);
+    mko_pubkey_from_seed(seed, pk);
+}
+
 /* public keys of indices first .. first+n-1 (full sign bit) */
 EXPORT void mko_derive(const u8 key[32], u32 src, u64 first, u64 n, u8* out) {
     oracle_init();
-    for (u64 i = 0; i < n; i++) {
-        u8 seed[32];
-        mko_seed(key, src, first + i, seed);
-        mko_pubkey_from_seed(seed, out + 32 * i);
-    }
-}
-
-/* incremental path: compressed (s0 + k)·B = s0·B + k·B for k = first .. first+n-1 */
-EXPORT void mko_incremental(const u8 s0[32], u64 first, u64 n, u8* out) {
-    oracle_init();
-    for (u64 i = 0; i < n; i++) {
-        u8 s[32];
-        u64 k = first + i, c = 0;
-        for (int b = 0; b < 32; b++) {
-            u64 add = b < 8 ? (k >> (8 * b)) & 0xff : 0;
-            c += (u64)s0[b] + add;
-            s[b] = (u8)c;
-            c >>= 8;
-        }
-        ge_compress(base_mul(s), out + 32 * i);
-    }
+    for (u64 i = 0; i < n; i++) index_pubkey(key, src, first + i, out + 32 * i);
 }
 
 /* ------------------------------------------------------------------------ */
@@ -532,9 +545,8 @@ EXPORT u64 mko_search(const u8 key[32], u32 src, u64 first, u64 n, const u8* nee
     oracle_init();
     u64 count = 0;
     for (u64 i = 0; i < n; i++) {
-        u8 seed[32], pk[32];
-        mko_seed(key, src, first + i, seed);
-        mko_pubkey_from_seed(seed, pk);
+        u8 pk[32];
+        index_pubkey(key, src, first + i, pk);
         pk[31] &= 0x7f;
         if (mko_match(pk, needle, len, fold, mode, 1)) {
             if (count < cap) hits[count] = first + i;

@@ -239,3 +239,88 @@ def test_longest_needle(gpu_ctx, oracle):
         job.launch(0, 1)
         hits, _ = job.hits()
     assert 123 in [i for i, _ in hits]
+
+
+# ---------------------------------------------------------------------------
+# incremental source: index k is the point (s0 + k)·B
+# ---------------------------------------------------------------------------
+
+def _start_scalar(seed_index: int, key_seed: int = 11) -> bytes:
+    """clamp(SHA-512(ChaCha20 seed `seed_index` of key SHA-256(u64 key_seed)))."""
+    from oracle import pyoracle
+    h = bytearray(hashlib.sha512(pyoracle.seed(chacha_key(key_seed), 0, seed_index)).digest()[:32])
+    h[0] &= 248
+    h[31] &= 127
+    h[31] |= 64
+    return bytes(h)
+
+
+@pytest.mark.parametrize("first,n", [(0, 1), (1, 7), (0, 4096), (2**32 - 5, 33), (2**40 + 1, 129),
+                                     (2**64 - 40, 40), (123457, 5000)])
+def test_incremental_derive_matches_oracle(gpu_ctx, oracle, first, n):
+    """Full public keys of the incremental source: the start point plus the thread's window
+    offset plus the step table, every key against the oracle's (s0 + k)·B."""
+    s0 = _start_scalar(0)
+    assert gpu_ctx.derive(s0, mk.SEED_INCREMENTAL, first, n) == oracle.derive(s0, 2, first, n)
+
+
+def test_incremental_start_is_seed_key(gpu_ctx, oracle):
+    """Key 0 of the start scalar clamp(SHA-512(seed)) is the seed's own Ed25519 public key."""
+    for i in (0, 5):
+        seed = oracle.seed(chacha_key(11), 0, i)
+        assert gpu_ctx.derive(_start_scalar(i), mk.SEED_INCREMENTAL, 0, 1) == oracle.pubkey(seed)
+
+
+def test_incremental_search_matches_oracle(gpu_ctx, oracle):
+    """Two full iterations of the incremental search kernel (the per-iteration jump of
+    keys_per_iter·B included) against the oracle, with a frequent needle so that tens of
+    thousands of indices are checked, and a 6-character suffix."""
+    s0 = _start_scalar(0)
+    kpi = gpu_ctx.keys_per_iter
+    base = 2**33 + 77
+    needles = [mk.Needle.contains("ab", case_sensitive=False), mk.Needle.suffix("Q", case_sensitive=True)]
+    with gpu_ctx.job(s0, mk.SEED_INCREMENTAL, needles) as job:
+        lowest = job.launch(base, 2)
+        hits, total = job.hits(cap=1 << 18)
+    assert total == len(hits)
+    want0 = oracle.search(s0, 2, base, 2 * kpi, b"ab", 2, True, 0)
+    want1 = oracle.search(s0, 2, base, 2 * kpi, b"Q", 1, False, 1)
+    assert [i for i, k in hits if k == 0] == want0
+    assert [i for i, k in hits if k == 1] == want1
+    assert len(want0) > 10000
+    assert lowest == min(want0 + want1)
+
+
+def test_incremental_rejects_large_start(gpu_ctx):
+    """The start scalar must be below 2^255 (s0 + k then never wraps)."""
+    bad = bytes(31) + b"\x80"
+    with pytest.raises(mk.GpuError) as e:
+        gpu_ctx.derive(bad, mk.SEED_INCREMENTAL, 0, 1)
+    assert e.value.status == mk._lib.ERR_BAD_ARG
+    with pytest.raises(mk.GpuError):
+        gpu_ctx.job(bad, mk.SEED_INCREMENTAL, [mk.Needle.contains("ab")])
+
+
+@pytest.mark.parametrize("source", [mk.SEED_CHACHA20, mk.SEED_COUNTER, mk.SEED_INCREMENTAL])
+def test_confirm_rederives_and_matches(gpu_ctx, oracle, source):
+    """Host confirmation (gpu.rs:973-996): every candidate is re-derived on the host; the public
+    key equals the oracle's, the secret is the seed (or s0 + index), and `matched` is the
+    sign-known test, so candidates that only matched through the other x sign are rejected."""
+    key = _start_scalar(3) if source == mk.SEED_INCREMENTAL else chacha_key(21)
+    needle = "Ab"
+    with gpu_ctx.job(key, source, [mk.Needle.contains(needle, case_sensitive=False)]) as job:
+        job.launch(2**36 + 5, 1)
+        hits, total = job.hits(cap=1 << 18)
+        assert 0 < len(hits) == total
+        sample = hits[:400]
+        results = [job.confirm(i, k) for i, k in sample]
+    rejected = 0
+    for (index, _), (ok, pk, secret) in zip(sample, results):
+        assert pk == oracle.derive(key, source, index, 1)
+        if source == mk.SEED_INCREMENTAL:
+            assert int.from_bytes(secret, "little") == int.from_bytes(key, "little") + index
+        else:
+            assert secret == oracle.seed(key, source, index)
+        assert ok == oracle.match(pk, b"ab", 2, True, 0, False)
+        rejected += not ok
+    assert rejected > 0  # sign-dependent candidates exist at this sample size

@@ -152,3 +152,46 @@ def test_reference_table_digits(oracle):
             half = 1 << (w - 1)
             assert all(-half <= d < half for d in out[:-1])
             assert 0 <= out[-1] <= half
+
+
+def _clamp(h: bytes) -> bytes:
+    s = bytearray(h[:32])
+    s[0] &= 248
+    s[31] &= 127
+    s[31] |= 64
+    return bytes(s)
+
+
+def test_incremental_oracle_pins(oracle):
+    """Incremental path (P_k = P_0 + k·B): key 0 of the start scalar clamp(SHA-512(seed)) is the
+    seed's Ed25519 public key, and P_0 + B + ... + B built with plain Python affine Edwards
+    additions gives the oracle's keys k = 0..40 (an independent restatement of the point sum)."""
+    p = 2**255 - 19
+    d = (-121665 * pow(121666, p - 2, p)) % p
+    inv = lambda v: pow(v, p - 2, p)  # noqa: E731
+
+    def add(P, Q):
+        (x1, y1), (x2, y2) = P, Q
+        t = d * x1 * x2 * y1 * y2 % p
+        return ((x1 * y2 + y1 * x2) * inv(1 + t) % p, (y1 * y2 + x1 * x2) * inv(1 - t) % p)
+
+    def compress(P):
+        x, y = P
+        return (y | (x & 1) << 255).to_bytes(32, "little")
+
+    key = chacha_key(11)
+    for index in (0, 1, 977):
+        seed = oracle.seed(key, 0, index)
+        s0 = _clamp(hashlib.sha512(seed).digest())
+        assert oracle.derive(s0, 2, 0, 1) == oracle.pubkey(seed)
+        B = oracle.point_affine(1)
+        P = oracle.point_affine(int.from_bytes(s0, "little"))
+        got = oracle.derive(s0, 2, 0, 41)
+        for k in range(41):
+            assert got[32 * k:32 * k + 32] == compress(P), (index, k)
+            P = add(P, B)
+    # far indices: key k of s0 is key 0 of s0 + k
+    s0 = _clamp(hashlib.sha512(oracle.seed(key, 0, 0)).digest())
+    for k in (2**32 - 1, 2**40 + 3, 2**64 - 1):
+        sk = (int.from_bytes(s0, "little") + k).to_bytes(32, "little")
+        assert oracle.derive(s0, 2, k, 1) == oracle.derive(sk, 2, 0, 1) == oracle.base_mul(sk)
