@@ -39,7 +39,29 @@ ALPHABET = "ABCDEFGHIJKLMNOPQRSTUVWXYZabcdefghijklmnopqrstuvwxyz0123456789+/"
 WORKLOADS = {
     "secure": {"total": 1 << 34, "step": 1 << 30, "source": 0, "seed": 7, "length": 7, "mode": "contains"},
     "incremental": {"total": 1 << 32, "step": 1 << 28, "source": 2, "seed": 11, "length": 6, "mode": "suffix"},
+    "multi": {"total": 1 << 34, "step": 1 << 30, "source": 0, "seed": 23, "length": 0, "mode": "mixed",
+              "launches": 4},
 }
+
+# the multi-pattern workload's regexes: DFAs of 6..57 states (mk_regex_compile), each matching
+# a random key with probability 2e-7 .. 1.4e-4 (exact, by propagating a uniform character
+# distribution through the DFA), 4.1e-4 together
+MULTI_REGEXES = ["(ab|cd|ef)[+/]x", "(?:aa|bb)(?:cc|dd)$", "x.{2}y.{2}z", "(?:ab|ba).{2}[0-9]{2}$",
+                 "z[0-9]{3}z", "(?:xyz|XYZ)$", "(?:AA|BB|CC)[0-9]{3}", "[ab].{4}[cd]z[0-9]"]
+
+
+def multi_patterns():
+    """64 text patterns: length uniform in 3..9 and characters uniform over the base64 alphabet
+    from numpy.random.default_rng(23); mode uniform over case-sensitive contains,
+    case-sensitive suffix and case-insensitive contains."""
+    import numpy as np
+    rng = np.random.default_rng(23)
+    out = []
+    for _ in range(64):
+        n = int(rng.integers(3, 10))
+        text = "".join(ALPHABET[int(v)] for v in rng.integers(0, 64, n))
+        out.append((text, ("contains", "suffix", "contains_ci")[int(rng.integers(0, 3))]))
+    return out
 
 
 def chacha20_seed0(key: bytes) -> bytes:
@@ -78,12 +100,22 @@ def workload_key(name: str = "secure") -> bytes:
 def workload_needle(name: str = "secure") -> str:
     import numpy as np
     w = WORKLOADS[name]
+    if name == "multi":
+        return ",".join(t for t, _ in multi_patterns()) + "," + ",".join(MULTI_REGEXES)
     rng = np.random.default_rng(w["seed"])
     return "".join(ALPHABET[int(i)] for i in rng.integers(0, 64, w["length"]))
 
 
 def workload_needles(name: str = "secure"):
     import meikey_b200 as mk
+    if name == "multi":
+        out = []
+        for text, mode in multi_patterns():
+            if mode == "suffix":
+                out.append(mk.Needle.suffix(text))
+            else:
+                out.append(mk.Needle.contains(text, case_sensitive=mode == "contains"))
+        return out + [mk.Needle.regex(r, max_states=64) for r in MULTI_REGEXES]
     n = workload_needle(name)
     return [mk.Needle.suffix(n) if WORKLOADS[name]["mode"] == "suffix" else mk.Needle.contains(n)]
 
@@ -276,7 +308,16 @@ def run_reference(args):
 
 
 def workload_config(workload, ctx, step_candidates=None, steps=None):
-    if workload == "incremental":
+    if workload == "multi":
+        cfg = {
+            "workload": "batched multi-pattern: secure-path ChaCha20 seeds (key SHA-256(u64 23)), 64 text "
+                        "patterns of length U{3..9} (numpy default_rng(23); case-sensitive contains, suffix, "
+                        "case-insensitive contains) + 8 regexes as DFAs of <= 64 states, one job, each step "
+                        "one CUDA-graph replay of 4 persistent launches; 2^34 candidates",
+            "candidates_total": WORKLOADS[workload]["total"],
+            "regexes": MULTI_REGEXES,
+        }
+    elif workload == "incremental":
         cfg = {
             "workload": "incremental (low-security) path: s0 = clamp(SHA-512(ChaCha20 seed 0 of key "
                         "SHA-256(u64 11))), P_k = P_0 + k*B by mixed additions, pooled inversion, base64, "
@@ -327,18 +368,28 @@ def run_ours(args):
     import meikey_b200 as mk
     wl = WORKLOADS[args.workload]
     key, needle, source = workload_key(args.workload), workload_needle(args.workload), wl["source"]
+    # the multi-pattern workload's 3-character patterns alone give ~1e-3 candidates per key
     ctx = mk.Context(device=local, table_rows=args.rows, keys_per_thread=args.kpt, block=args.block,
-                     self_check=True)
+                     self_check=True, hit_capacity=(1 << 22) if args.workload == "multi" else 0)
     kpi = ctx.keys_per_iter
-    iters = math.ceil((args.step_candidates or wl["step"]) / kpi)
-    step_keys = kpi * iters
+    launches = wl.get("launches", 1)  # > 1: a step is one replay of a CUDA graph of that many launches
+    iters = math.ceil((args.step_candidates or wl["step"]) / (kpi * launches))
+    step_keys = kpi * iters * launches
     rank_base = rank << 56
     peak, peak_lo = ctx.measure_mad_peaks()
     field_muls, mads_per_key = ctx.work_per_key(source)
-    job = ctx.job(key, source, workload_needles(args.workload))
+    needles = workload_needles(args.workload)
+    job = ctx.job(key, source, needles)
+    graph = job.graph(iters, launches) if launches > 1 else None
+
+    def enqueue_step(base):
+        if graph is not None:
+            graph.enqueue(base)
+        else:
+            job.enqueue(base, iters)
     # warm-up
     for w in range(args.warmup):
-        job.enqueue(rank_base + w * step_keys, iters)
+        enqueue_step(rank_base + w * step_keys)
     ctx.sync()
     # timed region: device-resident inputs, K launches back to back
     clocks = ClockSampler(local)
@@ -348,7 +399,7 @@ def run_ours(args):
     ctx.record(0)
     first = rank_base + args.warmup * step_keys
     for s in range(args.steps):
-        job.enqueue(first + s * step_keys, iters)
+        enqueue_step(first + s * step_keys)
     ctx.record(1)
     ctx.sync()
     dist.barrier()
@@ -367,17 +418,29 @@ def run_ours(args):
     t0 = time.perf_counter()
     for s in range(e2e_steps):
         with ctx.job(key, source, workload_needles(args.workload)) as j:
-            j.launch(first + (args.steps + s) * step_keys, iters)
-            hits, total = j.hits()
+            e2e_base = first + (args.steps + s) * step_keys
+            if launches > 1:
+                with j.graph(iters, launches) as g:
+                    g.launch(e2e_base)
+            else:
+                j.launch(e2e_base, iters)
+            hits, total = j.hits(cap=1 << 22)
             found += total
+            # one key per needle is written: confirm each needle's candidates in index order
+            # until one matches with its real x sign
+            done = set()
             for index, nd in hits:
-                confirmed += j.confirm(index, nd)[0]
+                if nd not in done and j.confirm(index, nd)[0]:
+                    done.add(nd)
+            confirmed += len(done)
             a, b = j.io_bytes()
             h2d += a
             d2h += b
     dt_e2e = time.perf_counter() - t0
     dt_e2e = dist.max(dt_e2e)
     e2e = step_keys * e2e_steps * world / dt_e2e
+    if graph is not None:
+        graph.close()
     job.close()
     ctx_info = dict(ctx.info)
     line = None
@@ -396,14 +459,16 @@ def run_ours(args):
             "kernel_ms_per_launch": ms_local / args.steps,
         }
         cfg = workload_config(args.workload, ctx, step_keys, args.steps)
+        cfg["launches_per_step"] = launches
+        cfg["needles"] = len(needles)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u32", "data": "synthetic", "config": cfg, "clocks": clk,
-            "gpu_launches": args.steps,
+            "gpu_launches": args.steps * launches,
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d // e2e_steps,
                     "d2h_bytes_per_step": d2h // e2e_steps, "steps": e2e_steps, "candidates": found,
-                    "confirmed_on_host": confirmed},
+                    "needles_confirmed_on_host": confirmed},
             "roofline": roofline,
             "device": ctx_info["name"],
         }

@@ -66,7 +66,7 @@ enum mk_mode { MK_MODE_CONTAINS = 0, MK_MODE_SUFFIX = 1, MK_MODE_REGEX = 2 };
  * table_rows chooses the comb geometry (rows of the fixed-base table: fewer rows
  * means fewer point additions per key and a larger table in HBM). */
 typedef struct mk_options {
-    uint32_t table_rows;      /* 10..16; default 12 */
+    uint32_t table_rows;      /* 10..20; default 12 */
     uint32_t keys_per_thread; /* keys one thread derives before the pooled inversion (default 16) */
     uint32_t block;           /* threads per CTA (default 512): 256 (keys per thread 4, 8, 16) or 512 (8, 16);
                                  the last warp of a search CTA only inverts */
@@ -108,9 +108,62 @@ typedef struct mk_info {
     char name[96];
 } mk_info;
 
+/* One candidate of the autotuner and what it measured. */
+typedef struct mk_tune_entry {
+    mk_options options;   /* the candidate (self_check is forced on) */
+    int status;           /* MK_OK, or why it was dropped (MK_ERR_SELF_CHECK, MK_ERR_OUT_OF_RANGE, ...) */
+    uint32_t stage;       /* the last stage it ran in: 1, or 2 for a finalist */
+    double keys_per_s;    /* its best measured secure-path rate */
+} mk_tune_entry;
+
+/* mk_search: where and how long one job searches. */
+typedef struct mk_search_config {
+    uint64_t first;          /* first index */
+    uint64_t max_tries;      /* indices to search before giving up (0 = no limit) */
+    double time_limit_s;     /* wall-clock limit checked between launches (0 = none) */
+    uint32_t iters;          /* iterations per launch (keys_per_iter each) */
+    uint32_t reserved;
+} mk_search_config;
+
+/* The outcome of mk_search: a host-verified key, or why there is none. */
+typedef struct mk_outcome {
+    int status;              /* MK_OK: key found; MK_ERR_STOPPED: budget, time limit or cancel */
+    uint32_t needle;         /* the needle the key matches */
+    uint64_t index;          /* its index */
+    uint64_t tries;          /* indices searched (Stats::tries) */
+    double elapsed_s;        /* Stats::elapsed */
+    uint8_t secret[32];      /* seed, or the scalar s0 + index of the incremental source */
+    uint8_t pk[32];          /* public key */
+} mk_outcome;
+
+/* Progress callback between launches (Progress, src/service/search.rs:33-40); nonzero cancels. */
+typedef int (*mk_progress_fn)(void* user, uint64_t tries, double elapsed_s);
+
+/* Continuous-batching server options. */
+typedef struct mk_server_options {
+    uint32_t max_jobs;       /* jobs admitted at once (needle slots, 1..128) */
+    uint32_t iters_per_tick; /* iterations per tick (one launch of iters_per_tick·keys_per_iter indices) */
+    uint64_t budget;         /* indices a job searches from its admission before it is censored */
+    uint64_t hit_capacity;   /* hit-ring entries the admitted jobs may plan for (0 = no limit) */
+} mk_server_options;
+
+/* A finished job of the server. */
+typedef struct mk_job_result {
+    uint64_t id;             /* the caller's id */
+    int status;              /* MK_OK found; MK_ERR_STOPPED censored at the budget */
+    uint32_t reserved;
+    uint64_t admit_index;    /* stream index at admission: the job searched [admit, admit + budget) */
+    uint64_t index;          /* the key's index (found) */
+    uint64_t tries;          /* indices searched for the job */
+    double expected_tries;   /* the estimate used for admission */
+    uint8_t secret[32];
+    uint8_t pk[32];
+} mk_job_result;
+
 typedef struct mk_ctx mk_ctx;
 typedef struct mk_job mk_job;
 typedef struct mk_graph mk_graph;
+typedef struct mk_server mk_server;
 
 /* Library ABI version (MK_ABI_VERSION). */
 MK_API uint32_t mk_abi_version(void);
@@ -161,6 +214,44 @@ MK_API int mk_graph_launch(mk_graph* graph, uint64_t base, int* found, uint64_t*
 MK_API int mk_graph_enqueue(mk_graph* graph, uint64_t base);
 MK_API void mk_graph_destroy(mk_graph* graph);
 
+/* Validates needles as mk_job_prepare would (host only, no device). */
+MK_API int mk_needles_check(const mk_needle* needles, uint32_t n_needles);
+/* keys_per_iter of the job's context */
+MK_API uint64_t mk_job_keys_per_iter(const mk_job* job);
+
+/* Expected number of indices to search until a key matches the needle (1 / the probability
+ * that a uniformly random key matches, computed exactly by propagating a uniform character
+ * distribution through the needle's DFA); INFINITY when it cannot match.  Host only. */
+MK_API double mk_expected_tries(const mk_needle* needle);
+
+/* Searcher::run for one job (src/service/search.rs:33-40 over gpu.rs:917-996): launches of
+ * cfg->iters iterations over cfg->first, first + keys_per_iter·iters, ...; after each launch
+ * its candidates are confirmed on the host in index order (mk_job_confirm) and the first
+ * that matches with its real x sign is returned: the lowest matching index of the range.
+ * Stops with status MK_ERR_STOPPED when max_tries indices are searched, the time limit passes
+ * or `progress` returns nonzero (checked between launches, so a cancel takes effect within
+ * one launch).  The return value is an error of the engine, else MK_OK. */
+MK_API int mk_search(mk_job* job, const mk_search_config* cfg, mk_progress_fn progress, void* user,
+                     mk_outcome* out);
+
+/* Continuous batching of many jobs over one candidate stream (no counterpart in the
+ * reference): every mk_server_tick is one launch over the next iters_per_tick·keys_per_iter
+ * indices of the stream (key, seed source) that tests the needles of all admitted jobs.
+ * Submitted jobs wait in a queue and are admitted at tick boundaries, shortest expected
+ * search first, while needle slots, the matcher's capacity and the hit-ring plan allow.
+ * A job admitted at stream index a searches [a, a + budget): its result is the lowest index
+ * there whose key matches (confirmed on the host), the same key mk_search finds for that
+ * needle alone from first = a; otherwise it is censored at the budget.  The server keeps a
+ * job of its own on the context; ticks are synchronous. */
+MK_API int mk_server_create(mk_ctx* ctx, const uint8_t key[32], int seed_source, const mk_server_options* options,
+                            uint64_t first, mk_server** out);
+MK_API int mk_server_submit(mk_server* server, const mk_needle* needle, uint64_t id);
+MK_API int mk_server_tick(mk_server* server, uint32_t* active, uint32_t* queued);
+/* Drains finished jobs (in completion order): writes up to cap results, *n = the number written. */
+MK_API int mk_server_results(mk_server* server, mk_job_result* out, uint32_t cap, uint32_t* n);
+MK_API uint64_t mk_server_position(const mk_server* server);
+MK_API void mk_server_destroy(mk_server* server);
+
 /* The host confirmation of a candidate (src/service/gpu.rs:973-996, confirm): re-derives
  * index `index` of the job's key stream on the CPU — the seed and its Ed25519 public key, or
  * for MK_SEED_INCREMENTAL the scalar s0 + index and (s0 + index)·B — and tests needle
@@ -194,6 +285,32 @@ MK_API int mk_derive(mk_ctx* ctx, const uint8_t key[32], int seed_source, uint64
  * from any thread or context on the same device, race on it. */
 MK_API int mk_derive_noalloc(mk_ctx* ctx, const uint8_t key[32], int seed_source, uint64_t first, uint64_t n,
                              uint8_t* out);
+
+/* Dfa::new + Dfa::gpu_table (src/model/pattern/dfa.rs:52-108, 189-200): compiles a regex
+ * into the DFA table of a MK_MODE_REGEX needle (states × 65 little-endian u16, state 0
+ * accepts, state 1 starts, column 64 flags acceptance at the end), for an unanchored search
+ * over the 43 characters after the key prefix.  Syntax: literals, `.`, classes with ranges
+ * and negation, \d, \w, escapes, groups, `|`, `*`, `+`, `?`, `{m}`, `{m,}`, `{m,n}`, `^`,
+ * `$`; case_sensitive = 0 matches letters in both cases.  `table` must hold
+ * max_states·130 bytes.  Returns MK_ERR_PATTERN (text in `err`) for a syntax error, a pattern
+ * that matches the empty string, or more than max_states states.  Needs no device. */
+MK_API int mk_regex_compile(const char* pattern, int case_sensitive, uint32_t max_states, uint8_t* table,
+                            uint32_t* states, char* err, size_t err_size);
+
+/* Staged autotuner (GpuOptions::fastest_staged, src/service/gpu.rs:302-393, 1016-1113):
+ * stage 1 creates a self-checked context per candidate (a variant whose keys differ from the
+ * host derivation is dropped) and times one launch of about trial_keys secure-path
+ * candidates; stage 2 re-times the `finalists` fastest in three rounds of alternating order.
+ * Writes every entry's status, stage and rate, and the index of the fastest to *best.
+ * MK_ERR_NO_SETTINGS when no candidate ran. */
+MK_API int mk_autotune(int device, mk_tune_entry* entries, uint32_t n, uint32_t finalists, uint64_t trial_keys,
+                       uint32_t* best);
+
+/* Field multiplications per second on the context's device in radix 2^32 (the search
+ * kernel's eight-limb field) and radix 2^25.5 (ten limbs, 100 mad.wide products), four
+ * independent chains per thread at full occupancy: the measurement behind the choice of
+ * limb radix (the search kernel is built for radix 2^32 only). */
+MK_API int mk_measure_field_mul(mk_ctx* ctx, double* radix32_per_s, double* radix26_per_s);
 
 /* Comb table entry (row, column) as 24 words (y+x, y-x, 2dxy; row 0 holds 2xy), for tests. */
 MK_API int mk_table_entry(mk_ctx* ctx, uint32_t row, uint64_t col, uint32_t out[24]);

@@ -50,6 +50,36 @@ class Options(ctypes.Structure):
     ]
 
 
+class TuneEntryC(ctypes.Structure):
+    _fields_ = [("options", Options), ("status", ctypes.c_int), ("stage", ctypes.c_uint32),
+                ("keys_per_s", ctypes.c_double)]
+
+
+class SearchConfigC(ctypes.Structure):
+    _fields_ = [("first", ctypes.c_uint64), ("max_tries", ctypes.c_uint64), ("time_limit_s", ctypes.c_double),
+                ("iters", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+
+
+class OutcomeC(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("needle", ctypes.c_uint32), ("index", ctypes.c_uint64),
+                ("tries", ctypes.c_uint64), ("elapsed_s", ctypes.c_double), ("secret", ctypes.c_uint8 * 32),
+                ("pk", ctypes.c_uint8 * 32)]
+
+
+class ServerOptionsC(ctypes.Structure):
+    _fields_ = [("max_jobs", ctypes.c_uint32), ("iters_per_tick", ctypes.c_uint32), ("budget", ctypes.c_uint64),
+                ("hit_capacity", ctypes.c_uint64)]
+
+
+class JobResultC(ctypes.Structure):
+    _fields_ = [("id", ctypes.c_uint64), ("status", ctypes.c_int), ("reserved", ctypes.c_uint32),
+                ("admit_index", ctypes.c_uint64), ("index", ctypes.c_uint64), ("tries", ctypes.c_uint64),
+                ("expected_tries", ctypes.c_double), ("secret", ctypes.c_uint8 * 32), ("pk", ctypes.c_uint8 * 32)]
+
+
+PROGRESS_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_double)
+
+
 class NeedleC(ctypes.Structure):
     _fields_ = [
         ("bytes", ctypes.POINTER(ctypes.c_uint8)),
@@ -116,6 +146,25 @@ SIGNATURES = [
                                            ctypes.POINTER(ctypes.c_double)]),
     ("mk_measure_mad_peaks", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
                                             ctypes.POINTER(ctypes.c_double)]),
+    ("mk_regex_compile", ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_uint32, ctypes.c_void_p,
+                                        ctypes.POINTER(ctypes.c_uint32), ctypes.c_char_p, ctypes.c_size_t]),
+    ("mk_autotune", ctypes.c_int, [ctypes.c_int, ctypes.POINTER(TuneEntryC), ctypes.c_uint32, ctypes.c_uint32,
+                                   ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint32)]),
+    ("mk_measure_field_mul", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
+                                            ctypes.POINTER(ctypes.c_double)]),
+    ("mk_needles_check", ctypes.c_int, [ctypes.POINTER(NeedleC), ctypes.c_uint32]),
+    ("mk_job_keys_per_iter", ctypes.c_uint64, [ctypes.c_void_p]),
+    ("mk_expected_tries", ctypes.c_double, [ctypes.POINTER(NeedleC)]),
+    ("mk_search", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(SearchConfigC), PROGRESS_FN, ctypes.c_void_p,
+                                 ctypes.POINTER(OutcomeC)]),
+    ("mk_server_create", ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(ServerOptionsC),
+                                        ctypes.c_uint64, ctypes.POINTER(ctypes.c_void_p)]),
+    ("mk_server_submit", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(NeedleC), ctypes.c_uint64]),
+    ("mk_server_tick", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint32)]),
+    ("mk_server_results", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(JobResultC), ctypes.c_uint32,
+                                         ctypes.POINTER(ctypes.c_uint32)]),
+    ("mk_server_position", ctypes.c_uint64, [ctypes.c_void_p]),
+    ("mk_server_destroy", None, [ctypes.c_void_p]),
     ("mk_derive_noalloc", ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_uint64,
                                          ctypes.c_uint64, ctypes.c_void_p]),
 ]

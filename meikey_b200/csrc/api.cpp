@@ -203,7 +203,7 @@ int mk_ctx_create(int device, const mk_options* options, mk_ctx** out) {
     if (!o.block) o.block = 512;
     const bool built = (o.block == 256 && (o.keys_per_thread == 4 || o.keys_per_thread == 8 || o.keys_per_thread == 16)) ||
                        (o.block == 512 && (o.keys_per_thread == 8 || o.keys_per_thread == 16));
-    if (o.table_rows < 10 || o.table_rows > 16 || !built || o.blocks_per_sm > 16 || o.hit_capacity > (1u << 26))
+    if (o.table_rows < 10 || o.table_rows > (uint32_t)mkb::MAX_ROWS || !built || o.blocks_per_sm > 16 || o.hit_capacity > (1u << 26))
         return MK_ERR_OUT_OF_RANGE;
     mk_ctx* c = new (std::nothrow) mk_ctx;
     if (!c) return MK_ERR_OUT_OF_MEMORY;
@@ -501,6 +501,15 @@ int mk_job_prepare(mk_ctx* c, const uint8_t key[32], int seed_source, const mk_n
     return MK_OK;
 }
 
+int mk_needles_check(const mk_needle* needles, uint32_t n_needles) {
+    std::unique_ptr<mkb::MatchSet> ms(new (std::nothrow) mkb::MatchSet);
+    if (!ms) return MK_ERR_OUT_OF_MEMORY;
+    std::vector<mkh25519::Needle> hosts;
+    return pack_needles(nullptr, needles, n_needles, *ms, hosts);
+}
+
+uint64_t mk_job_keys_per_iter(const mk_job* j) { return j && j->ctx ? j->ctx->info.keys_per_iter : 0; }
+
 int mk_job_update(mk_job* j, const mk_needle* needles, uint32_t n_needles) {
     if (!j) return MK_ERR_BAD_ARG;
     mk_ctx* c = j->ctx;
@@ -765,6 +774,13 @@ void mk_graph_destroy(mk_graph* g) {
     if (g->exec) cudaGraphExecDestroy(g->exec);
     if (g->graph) cudaGraphDestroy(g->graph);
     delete g;
+}
+
+int mk_measure_field_mul(mk_ctx* c, double* radix32_per_s, double* radix26_per_s) {
+    if (!c || !radix32_per_s || !radix26_per_s) return MK_ERR_BAD_ARG;
+    MK_CUDA(c, cudaSetDevice(c->device));
+    MK_CUDA(c, mkb::measure_field_mul_rates((int)c->info.sms, c->stream, radix32_per_s, radix26_per_s));
+    return MK_OK;
 }
 
 int mk_ctx_sync(mk_ctx* c) {

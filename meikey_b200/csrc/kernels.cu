@@ -823,6 +823,85 @@ cudaError_t measure_mad_peaks(int sms, cudaStream_t st, double* chain_per_s, dou
 
 }  // namespace mkb
 
+#include "fe26.cuh"
+
+namespace mkb {
+
+// Field-multiplication rate of the two limb radices: four independent chains a <- a·b per
+// thread, no memory traffic.  Radix 2^32 is the search kernel's field (fe32.cuh); radix
+// 2^25.5 (fe26.cuh, ten limbs, 100 mad.wide products) is the alternative the search is not
+// built for.
+template <int RADIX>
+__global__ void __launch_bounds__(256) k_fe_mul_rate(uint32_t iters, uint32_t seed, uint32_t* out) {
+    uint32_t sum = 0;
+    if (RADIX == 32) {
+        mk32::fe a[4], b;
+#pragma unroll
+        for (int i = 0; i < 8; i++) b.v[i] = seed * (i + 3) + threadIdx.x;
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+#pragma unroll
+            for (int i = 0; i < 8; i++) a[q].v[i] = threadIdx.x * 7 + q * 8 + i;
+        for (uint32_t it = 0; it < iters; it++)
+#pragma unroll
+            for (int q = 0; q < 4; q++) a[q] = mk32::fe_mul(a[q], b);
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+#pragma unroll
+            for (int i = 0; i < 8; i++) sum ^= a[q].v[i];
+    } else {
+        mk::fe a[4], b;
+#pragma unroll
+        for (int i = 0; i < 10; i++) b.v[i] = (seed * (i + 3) + threadIdx.x) & 0x1ffffffu;
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+#pragma unroll
+            for (int i = 0; i < 10; i++) a[q].v[i] = (threadIdx.x * 7 + q * 10 + i) & 0x1ffffffu;
+        for (uint32_t it = 0; it < iters; it++)
+#pragma unroll
+            for (int q = 0; q < 4; q++) a[q] = mk::fe_mul(a[q], b);
+#pragma unroll
+        for (int q = 0; q < 4; q++)
+#pragma unroll
+            for (int i = 0; i < 10; i++) sum ^= a[q].v[i];
+    }
+    out[(uint64_t)blockIdx.x * blockDim.x + threadIdx.x] = sum;
+}
+
+cudaError_t measure_field_mul_rates(int sms, cudaStream_t st, double* radix32_per_s, double* radix26_per_s) {
+    const uint32_t blocks = (uint32_t)sms * 8, threads = 256, iters = 1u << 11;
+    uint32_t* out = nullptr;
+    cudaError_t e = cudaMalloc(&out, sizeof(uint32_t) * blocks * threads);
+    if (e != cudaSuccess) return e;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    double best[2] = {0, 0};
+    k_fe_mul_rate<32><<<blocks, threads, 0, st>>>(iters / 16, 5u, out);
+    k_fe_mul_rate<26><<<blocks, threads, 0, st>>>(iters / 16, 5u, out);
+    for (int rep = 0; rep < 6 && e == cudaSuccess; rep++) {
+        const int r = rep & 1;
+        cudaEventRecord(e0, st);
+        if (r == 0) k_fe_mul_rate<32><<<blocks, threads, 0, st>>>(iters, 9u + rep, out);
+        else k_fe_mul_rate<26><<<blocks, threads, 0, st>>>(iters, 9u + rep, out);
+        cudaEventRecord(e1, st);
+        e = cudaEventSynchronize(e1);
+        if (e == cudaSuccess) e = cudaGetLastError();
+        float ms = 0;
+        if (e == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+        const double muls = (double)blocks * threads * iters * 4;
+        if (ms > 0 && muls / (ms * 1e-3) > best[r]) best[r] = muls / (ms * 1e-3);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(out);
+    *radix32_per_s = best[0];
+    *radix26_per_s = best[1];
+    return e;
+}
+
+}  // namespace mkb
+
 // ---------------------------------------------------------------------------
 // Derive without allocation: fixed device staging for mk_derive_noalloc
 // ---------------------------------------------------------------------------

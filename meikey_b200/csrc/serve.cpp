@@ -1,0 +1,375 @@
+// Host loops above the launch engine:
+//
+//   mk_search       the searcher of one job (Searcher::run over Engine, src/service/search.rs:33-40,
+//                   src/service/gpu.rs:917-996): launches over consecutive ranges, confirms
+//                   candidates on the host in index order, honours a tries budget, a time
+//                   limit and a cancel request from the progress callback, returns only a
+//                   host-verified key.
+//   mk_server_*     continuous batching of many jobs (no counterpart in the reference): one
+//                   candidate stream, every tick one launch that tests the needles of all
+//                   admitted jobs; jobs are admitted at tick boundaries as needle slots and
+//                   hit-ring memory free up, shortest expected search first.  A job admitted
+//                   at stream index a searches [a, a + budget): its result is the lowest
+//                   index there whose key matches (confirmed on the host), which is exactly
+//                   what mk_search of the same job from index a finds alone.
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <chrono>
+#include <deque>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/meikey_b200.h"
+
+namespace {
+
+double now_s() {
+    using namespace std::chrono;
+    return duration<double>(steady_clock::now().time_since_epoch()).count();
+}
+
+// Probability that a uniformly random key matches a DFA table over the 43 searched
+// characters (the first of them takes 16 values, the others 64): the state distribution
+// propagated character by character.
+double dfa_match_probability(const uint8_t* table, uint32_t states) {
+    std::vector<double> d(states, 0.0), nd(states);
+    d[1 % states] = 1.0;
+    auto next = [&](uint32_t s, uint32_t v) {
+        size_t at = ((size_t)s * 65 + v) * 2;
+        return (uint32_t)table[at] | (uint32_t)table[at + 1] << 8;
+    };
+    for (int pos = 0; pos < 43; pos++) {
+        std::fill(nd.begin(), nd.end(), 0.0);
+        const uint32_t values = pos == 0 ? 16 : 64;
+        for (uint32_t s = 0; s < states; s++) {
+            if (d[s] == 0.0) continue;
+            const double w = d[s] / values;
+            for (uint32_t v = 0; v < values; v++) nd[next(s, v)] += w;
+        }
+        d.swap(nd);
+    }
+    double p = d[0];
+    for (uint32_t s = 1; s < states; s++)
+        if (next(s, 64)) p += d[s];
+    return p;
+}
+
+// All hits of the job's last launch (sorted by index).
+int fetch_hits(mk_job* job, std::vector<mk_hit>& hits) {
+    uint32_t written = 0;
+    uint64_t total = 0;
+    int st = mk_job_hits(job, nullptr, 0, &written, &total);
+    if (st != MK_OK) return st;
+    hits.resize(total);
+    st = mk_job_hits(job, hits.data(), (uint32_t)total, &written, &total);
+    if (st != MK_OK) return st;
+    hits.resize(written);
+    return MK_OK;
+}
+
+}  // namespace
+
+extern "C" double mk_expected_tries(const mk_needle* nd) {
+    if (!nd || !nd->bytes || nd->len == 0) return 0.0;
+    if (nd->mode == MK_MODE_REGEX) {
+        double p = dfa_match_probability(nd->bytes, nd->len);
+        return p > 0 ? 1.0 / p : INFINITY;
+    }
+    // text needles: the DFA of the escaped needle (suffix: anchored at the end)
+    std::string rx;
+    for (uint32_t i = 0; i < nd->len; i++) {
+        char ch = (char)nd->bytes[i];
+        if (ch == '+' || ch == '/') rx += '\\';
+        rx += ch;
+    }
+    if (nd->mode == MK_MODE_SUFFIX) rx += '$';
+    std::vector<uint8_t> table(4096 * 130);
+    uint32_t states = 0;
+    if (mk_regex_compile(rx.c_str(), nd->fold ? 0 : 1, 4096, table.data(), &states, nullptr, 0) != MK_OK) return 0.0;
+    double p = dfa_match_probability(table.data(), states);
+    return p > 0 ? 1.0 / p : INFINITY;
+}
+
+extern "C" int mk_search(mk_job* job, const mk_search_config* cfg, mk_progress_fn progress, void* user,
+                         mk_outcome* out) {
+    if (!job || !cfg || !out || cfg->iters == 0) return MK_ERR_BAD_ARG;
+    memset(out, 0, sizeof *out);
+    const double t0 = now_s();
+    const uint64_t kpi = mk_job_keys_per_iter(job);
+    if (kpi == 0) return MK_ERR_BAD_ARG;
+    const uint64_t end = cfg->max_tries ? cfg->first + cfg->max_tries : ~0ull;
+    uint64_t base = cfg->first;
+    std::vector<mk_hit> hits;
+    for (;;) {
+        const uint64_t left = end - base;
+        const uint64_t want = (left + kpi - 1) / kpi;
+        const uint32_t iters = (uint32_t)std::min<uint64_t>(cfg->iters, want);
+        int found = 0;
+        uint64_t lowest = 0;
+        int st = mk_job_launch(job, base, iters, &found, &lowest);
+        if (st != MK_OK && st != MK_ERR_STOPPED) return st;
+        const uint64_t span = kpi * iters;
+        if (found) {
+            if (int e = fetch_hits(job, hits)) return e;
+            const uint32_t written = (uint32_t)hits.size();
+            for (uint32_t k = 0; k < written; k++) {
+                const mk_hit& h = hits[k];
+                if (h.index < base || h.index >= end) continue;
+                int ok = 0;
+                st = mk_job_confirm(job, h.index, h.needle, out->pk, out->secret, &ok);
+                if (st != MK_OK) return st;
+                if (ok) {
+                    out->status = MK_OK;
+                    out->index = h.index;
+                    out->needle = h.needle;
+                    out->tries = h.index - cfg->first + 1;
+                    out->elapsed_s = now_s() - t0;
+                    return MK_OK;
+                }
+            }
+        }
+        base += span;
+        out->tries = std::min(base, end) - cfg->first;
+        out->elapsed_s = now_s() - t0;
+        if (base >= end) {
+            out->status = MK_ERR_STOPPED;  // budget spent without a confirmed key
+            return MK_OK;
+        }
+        if (cfg->time_limit_s > 0 && out->elapsed_s >= cfg->time_limit_s) {
+            out->status = MK_ERR_STOPPED;
+            return MK_OK;
+        }
+        if (progress && progress(user, out->tries, out->elapsed_s)) {
+            out->status = MK_ERR_STOPPED;  // cancelled
+            return MK_OK;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// continuous batching
+// ---------------------------------------------------------------------------
+
+namespace {
+
+struct ServedJob {
+    uint64_t id = 0;
+    uint32_t mode = 0, fold = 0;
+    std::vector<uint8_t> bytes;
+    uint32_t len = 0;
+    double expected = 0;     // expected tries
+    uint64_t admit = 0;      // stream index at admission
+    uint64_t submitted_seq = 0;
+};
+
+}  // namespace
+
+struct mk_server {
+    mk_ctx* ctx = nullptr;
+    mk_job* job = nullptr;
+    mk_server_options opt{};
+    uint64_t pos = 0;         // next stream index
+    uint64_t kpi = 0;
+    uint64_t seq = 0;
+    std::deque<ServedJob> queued;
+    std::vector<ServedJob> active;  // slot order = needle order of the launch
+    std::vector<mk_job_result> done;
+    std::vector<mk_hit> hits;
+    bool needles_dirty = true;
+};
+
+static void to_needle(const ServedJob& j, mk_needle& nd) {
+    nd.bytes = j.bytes.data();
+    nd.len = j.len;
+    nd.fold = j.fold;
+    nd.mode = j.mode;
+}
+
+extern "C" int mk_server_create(mk_ctx* ctx, const uint8_t key[32], int seed_source, const mk_server_options* options,
+                                uint64_t first, mk_server** out) {
+    if (!ctx || !key || !options || !out) return MK_ERR_BAD_ARG;
+    const mk_server_options& o = *options;
+    if (o.max_jobs == 0 || o.max_jobs > 128 || o.iters_per_tick == 0 || o.budget == 0) return MK_ERR_OUT_OF_RANGE;
+    *out = nullptr;
+    std::unique_ptr<mk_server> s(new (std::nothrow) mk_server);
+    if (!s) return MK_ERR_OUT_OF_MEMORY;
+    s->ctx = ctx;
+    s->opt = o;
+    s->pos = first;
+    s->kpi = mk_keys_per_iter(ctx);
+    int st = mk_job_prepare(ctx, key, seed_source, nullptr, 0, 0, &s->job);
+    if (st != MK_OK) return st;
+    *out = s.release();
+    return MK_OK;
+}
+
+extern "C" void mk_server_destroy(mk_server* s) {
+    if (!s) return;
+    mk_job_destroy(s->job);
+    delete s;
+}
+
+extern "C" int mk_server_submit(mk_server* s, const mk_needle* nd, uint64_t id) {
+    if (!s || !nd || !nd->bytes || nd->len == 0) return MK_ERR_BAD_ARG;
+    ServedJob j;
+    j.id = id;
+    j.mode = nd->mode;
+    j.fold = nd->fold;
+    j.len = nd->len;
+    const size_t bytes = nd->mode == MK_MODE_REGEX ? (size_t)nd->len * 130 : nd->len;
+    j.bytes.assign(nd->bytes, nd->bytes + bytes);
+    // the needle must be valid on its own (checked now, so a bad one never blocks a tick)
+    if (int st = mk_needles_check(nd, 1)) return st;
+    j.expected = mk_expected_tries(nd);
+    j.submitted_seq = s->seq++;
+    s->queued.push_back(std::move(j));
+    return MK_OK;
+}
+
+// candidates expected per tick for a job (x sign unknown doubles the rate at worst)
+static double hits_per_tick(const mk_server* s, const ServedJob& j) {
+    const double span = (double)s->kpi * s->opt.iters_per_tick;
+    return j.expected > 0 ? 2.0 * span / j.expected : span;
+}
+
+static int admit(mk_server* s) {
+    if (s->queued.empty()) return MK_OK;
+    // shortest expected search first; ties in submission order
+    std::stable_sort(s->queued.begin(), s->queued.end(),
+                     [](const ServedJob& a, const ServedJob& b) { return a.expected < b.expected; });
+    double ring = 0;
+    for (auto& a : s->active) ring += 4.0 * hits_per_tick(s, a) + 64.0;
+    std::vector<mk_needle> nds;
+    for (auto it = s->queued.begin(); it != s->queued.end();) {
+        if (s->active.size() >= s->opt.max_jobs) break;
+        const double need = 4.0 * hits_per_tick(s, *it) + 64.0;
+        if (s->opt.hit_capacity && ring + need > s->opt.hit_capacity) {
+            ++it;  // waits until hit-ring memory frees up
+            continue;
+        }
+        // does it still fit the matcher's shift-and state / regex slots?
+        nds.clear();
+        for (auto& a : s->active) {
+            mk_needle nd;
+            to_needle(a, nd);
+            nds.push_back(nd);
+        }
+        mk_needle nd;
+        to_needle(*it, nd);
+        nds.push_back(nd);
+        if (mk_needles_check(nds.data(), (uint32_t)nds.size()) != MK_OK) {
+            ++it;
+            continue;
+        }
+        ServedJob j = std::move(*it);
+        it = s->queued.erase(it);
+        j.admit = s->pos;
+        ring += need;
+        s->active.push_back(std::move(j));
+        s->needles_dirty = true;
+    }
+    return MK_OK;
+}
+
+static void finish(mk_server* s, size_t slot, int status, uint64_t index, uint64_t tries, const uint8_t* pk,
+                  const uint8_t* secret) {
+    const ServedJob& j = s->active[slot];
+    mk_job_result r{};
+    r.id = j.id;
+    r.status = status;
+    r.admit_index = j.admit;
+    r.index = index;
+    r.tries = tries;
+    r.expected_tries = j.expected;
+    if (pk) memcpy(r.pk, pk, 32);
+    if (secret) memcpy(r.secret, secret, 32);
+    s->done.push_back(r);
+}
+
+extern "C" int mk_server_tick(mk_server* s, uint32_t* active, uint32_t* queued) {
+    if (!s) return MK_ERR_BAD_ARG;
+    int st = admit(s);
+    if (st) return st;
+    if (s->active.empty()) {
+        if (active) *active = 0;
+        if (queued) *queued = (uint32_t)s->queued.size();
+        return MK_OK;
+    }
+    std::vector<mk_needle> nds(s->active.size());
+    for (size_t k = 0; k < s->active.size(); k++) to_needle(s->active[k], nds[k]);
+    if (s->needles_dirty) {
+        st = mk_job_update(s->job, nds.data(), (uint32_t)nds.size());
+        if (st) return st;
+        s->needles_dirty = false;
+    }
+    // one tick over [pos, pos + span); a hit-ring overflow re-runs the range in halves
+    const uint64_t span = s->kpi * s->opt.iters_per_tick;
+    std::vector<mk_hit> hits;
+    std::vector<std::pair<uint64_t, uint32_t>> todo{{s->pos, s->opt.iters_per_tick}};
+    while (!todo.empty()) {
+        auto [b, it] = todo.back();
+        todo.pop_back();
+        int found = 0;
+        uint64_t lowest = 0;
+        st = mk_job_launch(s->job, b, it, &found, &lowest);
+        if (st == MK_ERR_HIT_RING_FULL && it > 1) {
+            todo.push_back({b + s->kpi * (it / 2), it - it / 2});
+            todo.push_back({b, it / 2});
+            continue;
+        }
+        if (st != MK_OK) return st;
+        if (!found) continue;
+        std::vector<mk_hit> part;
+        if (int e = fetch_hits(s->job, part)) return e;
+        hits.insert(hits.end(), part.begin(), part.end());
+    }
+    std::sort(hits.begin(), hits.end(),
+              [](const mk_hit& a, const mk_hit& b) { return a.index != b.index ? a.index < b.index : a.needle < b.needle; });
+    // per job, in index order: the first candidate that matches with its real x sign
+    std::vector<char> closed(s->active.size(), 0);
+    uint8_t pk[32], secret[32];
+    for (const mk_hit& h : hits) {
+        const size_t k = h.needle;
+        if (k >= s->active.size() || closed[k]) continue;
+        const ServedJob& j = s->active[k];
+        if (h.index < j.admit || h.index >= j.admit + s->opt.budget) continue;
+        int ok = 0;
+        st = mk_job_confirm(s->job, h.index, h.needle, pk, secret, &ok);
+        if (st != MK_OK) return st;
+        if (ok) {
+            finish(s, k, MK_OK, h.index, h.index - j.admit + 1, pk, secret);
+            closed[k] = 1;
+        }
+    }
+    s->pos += span;
+    for (size_t k = 0; k < s->active.size(); k++) {
+        const ServedJob& j = s->active[k];
+        if (!closed[k] && s->pos >= j.admit + s->opt.budget) {
+            finish(s, k, MK_ERR_STOPPED, 0, s->opt.budget, nullptr, nullptr);  // censored at the budget
+            closed[k] = 1;
+        }
+    }
+    size_t w = 0;
+    for (size_t k = 0; k < s->active.size(); k++)
+        if (!closed[k]) s->active[w++] = std::move(s->active[k]);
+    if (w != s->active.size()) s->needles_dirty = true;
+    s->active.resize(w);
+    if (active) *active = (uint32_t)s->active.size();
+    if (queued) *queued = (uint32_t)s->queued.size();
+    return MK_OK;
+}
+
+extern "C" int mk_server_results(mk_server* s, mk_job_result* out, uint32_t cap, uint32_t* n) {
+    if (!s || !n || (cap && !out)) return MK_ERR_BAD_ARG;
+    const uint32_t k = (uint32_t)std::min<size_t>(cap, s->done.size());
+    for (uint32_t i = 0; i < k; i++) out[i] = s->done[i];
+    s->done.erase(s->done.begin(), s->done.begin() + k);
+    *n = k;
+    return MK_OK;
+}
+
+extern "C" uint64_t mk_server_position(const mk_server* s) { return s ? s->pos : 0; }

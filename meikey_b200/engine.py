@@ -44,8 +44,26 @@ class Needle:
     def dfa(table: bytes, states: int) -> "Needle":
         return Needle(bytes(table), L.MODE_REGEX, False, states)
 
+    @staticmethod
+    def regex(pattern: str, case_sensitive: bool = True, max_states: int = 4096) -> "Needle":
+        """A regex needle compiled by the library (mk_regex_compile)."""
+        lib = L.load()
+        table = ctypes.create_string_buffer(max_states * 130)
+        states = ctypes.c_uint32()
+        err = ctypes.create_string_buffer(256)
+        st = lib.mk_regex_compile(pattern.encode(), 1 if case_sensitive else 0, max_states, table,
+                                  ctypes.byref(states), err, 256)
+        if st != L.OK:
+            raise GpuError(st, err.value.decode(errors="replace"))
+        return Needle.dfa(table.raw[:states.value * 130], states.value)
+
     def c_len(self) -> int:
         return self.states if self.mode == L.MODE_REGEX else len(self.text)
+
+    def expected_tries(self) -> float:
+        """1 / probability that a random key matches (mk_expected_tries)."""
+        arr, keep = _needle_array([self])
+        return float(L.load().mk_expected_tries(arr))
 
 
 def _check(lib, ctx_ptr, status: int):
@@ -117,6 +135,12 @@ class Context:
         """(carry-chain row MADs/s, plain mad.lo MADs/s) of the device (bounded microbenchmarks)."""
         a, b = ctypes.c_double(), ctypes.c_double()
         _check(self._lib, self._ptr, self._lib.mk_measure_mad_peaks(self._ptr, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def measure_field_mul(self):
+        """(radix-2^32, radix-2^25.5) field multiplications per second of the device."""
+        a, b = ctypes.c_double(), ctypes.c_double()
+        _check(self._lib, self._ptr, self._lib.mk_measure_field_mul(self._ptr, ctypes.byref(a), ctypes.byref(b)))
         return a.value, b.value
 
     def sync(self):
@@ -202,6 +226,20 @@ class Job:
         """A CUDA graph of `launches` launches of `iters` iterations each (mk_job_graph_create)."""
         return Graph(self, iters, launches)
 
+    def search(self, first: int = 0, max_tries: int = 0, iters: int = 16, time_limit_s: float = 0.0,
+               progress=None) -> dict:
+        """Searcher::run (mk_search): the lowest host-confirmed match from `first`, or status
+        STOPPED after max_tries indices, the time limit, or `progress(tries, elapsed)` returning
+        True (checked between launches)."""
+        cfg = L.SearchConfigC(first, max_tries, time_limit_s, iters, 0)
+        out = L.OutcomeC()
+        cb = L.PROGRESS_FN((lambda user, tries, el: 1 if progress(int(tries), float(el)) else 0)
+                           if progress else (lambda user, tries, el: 0))
+        _check(self._lib, self.ctx._ptr, self._lib.mk_search(self._ptr, ctypes.byref(cfg), cb, None, ctypes.byref(out)))
+        return {"status": out.status, "found": out.status == L.OK, "index": int(out.index), "needle": int(out.needle),
+                "tries": int(out.tries), "elapsed_s": float(out.elapsed_s), "secret": bytes(out.secret),
+                "pk": bytes(out.pk)}
+
     def confirm(self, index: int, needle: int):
         """Host confirmation of a candidate: (matched, public key, secret).  The secret is the
         seed (ChaCha20 / counter sources) or the scalar s0 + index (incremental source)."""
@@ -265,6 +303,92 @@ class Graph:
     def close(self):
         if self._ptr:
             self._lib.mk_graph_destroy(self._ptr)
+            self._ptr = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# keys/thread x block variants the library is built for
+BUILT_VARIANTS = [(4, 256), (8, 256), (16, 256), (8, 512), (16, 512)]
+
+
+def tune_space(rows=(11, 12, 13, 14, 16), variants=BUILT_VARIANTS, blocks_per_sm=(0,)):
+    """Candidate options: comb rows (table size against multiplications per key) x keys per
+    thread and block (inversion batch = keys per thread x compute warps) x CTAs per SM."""
+    return [dict(table_rows=r, keys_per_thread=k, block=b, blocks_per_sm=s)
+            for r in rows for (k, b) in variants for s in blocks_per_sm]
+
+
+def autotune(device: int = 0, candidates=None, finalists: int = 3, trial_keys: int = 1 << 27):
+    """Runs mk_autotune; returns (best options dict, per-candidate results)."""
+    lib = L.load()
+    cands = candidates or tune_space()
+    arr = (L.TuneEntryC * len(cands))()
+    for i, c in enumerate(cands):
+        arr[i].options = L.Options(c["table_rows"], c["keys_per_thread"], c["block"], c.get("blocks_per_sm", 0), 1, 0)
+    best = ctypes.c_uint32()
+    st = lib.mk_autotune(device, arr, len(cands), finalists, trial_keys, ctypes.byref(best))
+    if st != L.OK:
+        raise GpuError(st, "autotune")
+    results = [dict(cands[i], status=arr[i].status, stage=arr[i].stage, keys_per_s=arr[i].keys_per_s)
+               for i in range(len(cands))]
+    return dict(cands[best.value]), results
+
+
+class Server:
+    """Continuous batching of many jobs over one candidate stream (mk_server_*)."""
+
+    def __init__(self, ctx: Context, key: bytes, source: int = L.SEED_CHACHA20, max_jobs: int = 64,
+                 iters_per_tick: int = 8, budget: int = 1 << 26, hit_capacity: int = 0, first: int = 0):
+        self.ctx = ctx
+        self._lib = ctx._lib
+        opts = L.ServerOptionsC(max_jobs, iters_per_tick, budget, hit_capacity)
+        ptr = ctypes.c_void_p()
+        _check(self._lib, ctx._ptr, self._lib.mk_server_create(ctx._ptr, bytes(key), source, ctypes.byref(opts), first,
+                                                               ctypes.byref(ptr)))
+        self._ptr = ptr
+
+    def submit(self, needle: Needle, job_id: int):
+        arr, keep = _needle_array([needle])
+        _check(self._lib, self.ctx._ptr, self._lib.mk_server_submit(self._ptr, arr, job_id))
+
+    def tick(self):
+        """One launch for all admitted jobs; returns (active, queued) after it."""
+        a, q = ctypes.c_uint32(), ctypes.c_uint32()
+        _check(self._lib, self.ctx._ptr, self._lib.mk_server_tick(self._ptr, ctypes.byref(a), ctypes.byref(q)))
+        return a.value, q.value
+
+    def results(self) -> List[dict]:
+        out = (L.JobResultC * 256)()
+        n = ctypes.c_uint32()
+        res = []
+        while True:
+            _check(self._lib, self.ctx._ptr, self._lib.mk_server_results(self._ptr, out, 256, ctypes.byref(n)))
+            for i in range(n.value):
+                r = out[i]
+                res.append({"id": int(r.id), "found": r.status == L.OK, "status": r.status,
+                            "admit_index": int(r.admit_index), "index": int(r.index), "tries": int(r.tries),
+                            "expected_tries": float(r.expected_tries), "secret": bytes(r.secret), "pk": bytes(r.pk)})
+            if n.value < 256:
+                return res
+
+    @property
+    def position(self) -> int:
+        return int(self._lib.mk_server_position(self._ptr))
+
+    def close(self):
+        if self._ptr:
+            self._lib.mk_server_destroy(self._ptr)
             self._ptr = ctypes.c_void_p()
 
     def __enter__(self):

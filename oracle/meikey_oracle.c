@@ -556,6 +556,23 @@ EXPORT u64 mko_search(const u8 key[32], u32 src, u64 first, u64 n, const u8* nee
     return count;
 }
 
+/* Candidate scan of n precomputed public keys pks (indices first .. first+n-1): the same
+ * sign-unknown test as mko_search, for checking many needles against one key range. */
+EXPORT u64 mko_match_keys(const u8* pks, u64 n, u64 first, const u8* needle, u32 len, u32 fold, u32 mode,
+                          u64* hits, u64 cap) {
+    u64 count = 0;
+    for (u64 i = 0; i < n; i++) {
+        u8 pk[32];
+        memcpy(pk, pks + 32 * i, 32);
+        pk[31] &= 0x7f;
+        if (mko_match(pk, needle, len, fold, mode, 1)) {
+            if (count < cap) hits[count] = first + i;
+            count++;
+        }
+    }
+    return count;
+}
+
 /* ------------------------------------------------------------------------ */
 /* the reference's packed comb table (for the reference kernel built on CPU)  */
 /* ------------------------------------------------------------------------ */

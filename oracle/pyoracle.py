@@ -47,6 +47,8 @@ def lib():
             "mko_match": (ctypes.c_int, [u8p, u8p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32]),
             "mko_search": (u64, [u8p, ctypes.c_uint32, u64, u64, u8p, ctypes.c_uint32, ctypes.c_uint32,
                                  ctypes.c_uint32, ctypes.c_void_p, u64]),
+            "mko_match_keys": (u64, [ctypes.c_void_p, u64, u64, u8p, ctypes.c_uint32, ctypes.c_uint32,
+                                     ctypes.c_uint32, ctypes.c_void_p, u64]),
             "mko_ref_table_words": (u64, [ctypes.c_uint32]),
             "mko_ref_table": (None, [ctypes.c_uint32, ctypes.c_void_p]),
             "mko_digits": (None, [u8p, ctypes.c_uint32, ctypes.c_void_p]),
@@ -139,6 +141,16 @@ def search(key: bytes, source: int, first: int, n: int, needle: bytes, length: i
     with ThreadPoolExecutor(threads) as ex:
         parts = list(ex.map(run, _chunks(first, n, threads * 4)))
     return sorted(i for p in parts for i in p)
+
+
+def match_keys(pks: bytes, first: int, needle: bytes, length: int, fold: bool, mode: int):
+    """Candidate indices among precomputed keys pks (index first + i for key i), sign unknown."""
+    n = len(pks) // 32
+    cap = n
+    hits = (ctypes.c_uint64 * max(1, cap))()
+    buf = ctypes.create_string_buffer(pks, len(pks))
+    k = lib().mko_match_keys(buf, n, first, needle, length, int(fold), mode, hits, cap)
+    return [hits[i] for i in range(min(k, cap))]
 
 
 def ref_table(width: int):

@@ -40,6 +40,7 @@ def test_struct_layouts_match_header():
     assert ctypes.sizeof(_lib.NeedleC) == 24
     assert ctypes.sizeof(_lib.HitC) == 16
     assert ctypes.sizeof(_lib.InfoC) == 4 * 6 + 16 + 96
+    assert ctypes.sizeof(_lib.TuneEntryC) == 24 + 4 + 4 + 8
 
 
 def test_bad_arguments_return_status():

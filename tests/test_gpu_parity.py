@@ -324,3 +324,112 @@ def test_confirm_rederives_and_matches(gpu_ctx, oracle, source):
         assert ok == oracle.match(pk, b"ab", 2, True, 0, False)
         rejected += not ok
     assert rejected > 0  # sign-dependent candidates exist at this sample size
+
+
+# ---------------------------------------------------------------------------
+# multi-pattern jobs, needle updates, CUDA graphs
+# ---------------------------------------------------------------------------
+
+def _multi_needles():
+    """The multi-pattern workload's 64 text patterns and 8 regexes (library-compiled DFAs)."""
+    import bench
+    return bench.workload_needles("multi")
+
+
+def _oracle_args(n):
+    if n.mode == mk.MODE_REGEX:
+        return n.text, n.states, False, 2
+    return n.text, len(n.text), n.fold, n.mode
+
+
+def test_multi_pattern_job_matches_each_pattern_alone(gpu_ctx, oracle):
+    """64 text patterns of length 3..9 (contains, suffix, case-insensitive) and 8 regex DFAs in
+    one launch: for every pattern, its hits are exactly the oracle's candidates for that
+    pattern alone over the same keys (multi-pattern semantics pinned pattern by pattern)."""
+    needles = _multi_needles()
+    key = chacha_key(23)
+    base = 2**44 + 3
+    n = gpu_ctx.keys_per_iter
+    with gpu_ctx.job(key, mk.SEED_CHACHA20, needles) as job:
+        job.launch(base, 1)
+        hits, total = job.hits(cap=1 << 18)
+    assert total == len(hits)
+    pks = oracle.derive(key, 0, base, n)
+    for k, nd in enumerate(needles):
+        want = oracle.match_keys(pks, base, *_oracle_args(nd))
+        assert [i for i, j in hits if j == k] == want, (k, nd.text[:12], nd.mode)
+
+
+def test_regex_needle_compiled_by_library(gpu_ctx, golden):
+    """A regex compiled by mk_regex_compile gives the golden candidate set of that regex."""
+    key = bytes.fromhex(golden["chacha_key"])
+    lo, hi = golden["search_range"]
+    for case in [c for c in golden["search"] if c["mode"] == 2]:
+        nd = mk.Needle.regex(case["regex"], case_sensitive=case["case_sensitive"])
+        with gpu_ctx.job(key, mk.SEED_CHACHA20, [nd]) as job:
+            job.launch(lo, 1)
+            hits, _ = job.hits()
+        assert [i for i, _ in hits if lo <= i < hi] == case["hits"], case["regex"]
+
+
+def test_job_update_equals_new_job(gpu_ctx):
+    """mk_job_update between launches: the updated job finds what a fresh job with those needles finds."""
+    key = chacha_key(8)
+    first = [mk.Needle.contains("Ab9")]
+    second = [mk.Needle.suffix("Q", case_sensitive=True), mk.Needle.contains("xyz", case_sensitive=False)]
+    with gpu_ctx.job(key, mk.SEED_CHACHA20, first) as job:
+        job.launch(0, 1)
+        a, _ = job.hits()
+        job.update(second)
+        job.launch(0, 1)
+        b, _ = job.hits()
+    with gpu_ctx.job(key, mk.SEED_CHACHA20, second) as fresh:
+        fresh.launch(0, 1)
+        want, _ = fresh.hits()
+    assert b == want and a != b
+
+
+@pytest.mark.parametrize("source", [mk.SEED_CHACHA20, mk.SEED_INCREMENTAL])
+def test_graph_replay_equals_launches(gpu_ctx, source):
+    """A CUDA graph of 3 launches of 2 iterations, replayed at two bases, gives the hits of the
+    same ranges searched by plain launches (kernel-node parameters updated per replay)."""
+    key = _start_scalar(1) if source == mk.SEED_INCREMENTAL else chacha_key(9)
+    kpi = gpu_ctx.keys_per_iter
+    nd = [mk.Needle.contains("Ab", case_sensitive=False)]
+    with gpu_ctx.job(key, source, nd) as job:
+        with job.graph(2, 3) as g:
+            assert g.span == 6 * kpi
+            for base in (0, 2**40 + 7):
+                lowest = g.launch(base)
+                got, total = job.hits(cap=1 << 18)
+                want = []
+                for r in range(3):
+                    job.launch(base + r * 2 * kpi, 2)
+                    want += job.hits(cap=1 << 18)[0]
+                assert got == sorted(want) and total == len(want)
+                assert lowest == got[0][0]
+
+
+# ---------------------------------------------------------------------------
+# autotuner and limb-radix measurement
+# ---------------------------------------------------------------------------
+
+def test_autotune_small_space():
+    """mk_autotune over four candidates (one outside the built variants): the invalid one is
+    dropped with its status, the rest are measured, and the winner is the fastest finalist."""
+    from meikey_b200.engine import autotune
+    cands = [dict(table_rows=13, keys_per_thread=16, block=512), dict(table_rows=12, keys_per_thread=8, block=256),
+             dict(table_rows=16, keys_per_thread=16, block=256), dict(table_rows=12, keys_per_thread=32, block=512)]
+    best, results = autotune(0, cands, finalists=2, trial_keys=1 << 24)
+    assert results[3]["status"] == mk._lib.ERR_OUT_OF_RANGE
+    ok = [r for r in results if r["status"] == 0]
+    assert len(ok) == 3 and all(r["keys_per_s"] > 1e7 for r in ok)
+    finalists = [r for r in ok if r["stage"] == 2]
+    assert len(finalists) == 2
+    top = max(finalists, key=lambda r: r["keys_per_s"])
+    assert best == {k: top[k] for k in best}
+
+
+def test_field_mul_rates(gpu_ctx):
+    r32, r26 = gpu_ctx.measure_field_mul()
+    assert r32 > 1e10 and r26 > 1e10

@@ -1,0 +1,113 @@
+"""GPU tests of the host loops: the single-job searcher (mk_search, the reference's
+Searcher::run over the engine, src/service/search.rs:33-40, gpu.rs:917-996) and the
+continuous-batching server (mk_server_*).  Keys are checked against the oracle; every
+server result must equal the same job searched alone from its admission index."""
+import random
+
+import pytest
+
+import meikey_b200 as mk
+from conftest import chacha_key
+
+pytestmark = pytest.mark.gpu
+
+ALPHABET = "ABCDEFGHIJKLMNOPQRSTUVWXYZabcdefghijklmnopqrstuvwxyz0123456789+/"
+
+
+def _first_full_match(oracle, key, source, first, last, needle):
+    """Lowest index in [first, last] whose full key (x sign known) matches, by the oracle."""
+    nb, n, fold, mode = needle.text, len(needle.text), needle.fold, needle.mode
+    for i in oracle.search(key, source, first, last - first + 1, nb, n, fold, mode):
+        if oracle.match(oracle.derive(key, source, i, 1), nb, n, fold, mode, False):
+            return i
+    return None
+
+
+@pytest.mark.parametrize("source", [mk.SEED_CHACHA20, mk.SEED_COUNTER])
+def test_search_returns_lowest_confirmed_key(gpu_ctx, oracle, source):
+    key = chacha_key(31 + source)
+    nd = mk.Needle.contains("Ab9")
+    with gpu_ctx.job(key, source, [nd]) as job:
+        out = job.search(first=12345, iters=1)
+    assert out["found"]
+    assert out["pk"] == oracle.derive(key, source, out["index"], 1)
+    assert out["secret"] == oracle.seed(key, source, out["index"])
+    assert out["tries"] == out["index"] - 12345 + 1
+    assert _first_full_match(oracle, key, source, 12345, out["index"], nd) == out["index"]
+
+
+def test_search_budget_and_cancel(gpu_ctx):
+    key = chacha_key(40)
+    kpi = gpu_ctx.keys_per_iter
+    nd = mk.Needle.contains("zzzzzzzzz")  # practically never matches
+    with gpu_ctx.job(key, mk.SEED_CHACHA20, [nd]) as job:
+        out = job.search(first=0, max_tries=3 * kpi + 5, iters=2)
+        assert not out["found"] and out["status"] == mk._lib.ERR_STOPPED
+        assert out["tries"] == 3 * kpi + 5
+        calls = []
+        out = job.search(first=0, iters=1, progress=lambda tries, el: calls.append(tries) or True)
+        assert not out["found"] and calls == [kpi] and out["tries"] == kpi
+
+
+def _random_needles(n, seed):
+    rng = random.Random(seed)
+    out = []
+    for _ in range(n):
+        length = rng.randint(3, 4)
+        text = "".join(rng.choice(ALPHABET) for _ in range(length))
+        mode = rng.randrange(3)
+        if mode == 1:
+            out.append(mk.Needle.suffix(text[:2]))
+        else:
+            out.append(mk.Needle.contains(text, case_sensitive=mode == 0))
+    return out
+
+
+def test_server_results_equal_jobs_alone(gpu_ctx, oracle):
+    """24 jobs (two of them practically unmatchable) through 16 slots: each job's result (found key or censoring) is the
+    result of the same needle searched alone from its admission index with a different launch
+    size, and found keys are the oracle's."""
+    key = chacha_key(31)
+    kpi = gpu_ctx.keys_per_iter
+    budget = 24 * kpi + 7
+    needles = _random_needles(22, 5) + [mk.Needle.contains("Zq9xYw7"), mk.Needle.suffix("Qz81a")]
+    results = {}
+    with mk.Server(gpu_ctx, key, max_jobs=16, iters_per_tick=2, budget=budget) as srv:
+        for i, nd in enumerate(needles):
+            srv.submit(nd, i)
+        for _ in range(200):
+            active, queued = srv.tick()
+            for r in srv.results():
+                results[r["id"]] = r
+            if len(results) == len(needles):
+                break
+    assert len(results) == len(needles)
+    assert any(r["found"] for r in results.values()) and any(not r["found"] for r in results.values())
+    admits = sorted({r["admit_index"] for r in results.values()})
+    assert len(admits) > 1  # some jobs waited for a slot
+    for i, nd in enumerate(needles):
+        r = results[i]
+        with gpu_ctx.job(key, mk.SEED_CHACHA20, [nd]) as job:
+            alone = job.search(first=r["admit_index"], max_tries=budget, iters=3)
+        assert alone["found"] == r["found"], i
+        if r["found"]:
+            assert (alone["index"], alone["pk"], alone["secret"]) == (r["index"], r["pk"], r["secret"]), i
+            assert r["pk"] == oracle.derive(key, 0, r["index"], 1)
+        else:
+            assert r["tries"] == budget
+
+
+def test_server_admits_shortest_expected_first(gpu_ctx):
+    """With one slot, the queued job with the smaller expected search is admitted first."""
+    key = chacha_key(32)
+    long_job = mk.Needle.contains("Zq9x")
+    short_job = mk.Needle.contains("ab", case_sensitive=False)
+    assert short_job.expected_tries() < long_job.expected_tries()
+    with mk.Server(gpu_ctx, key, max_jobs=1, iters_per_tick=1, budget=gpu_ctx.keys_per_iter) as srv:
+        srv.submit(long_job, 1)
+        srv.submit(short_job, 2)
+        srv.tick()
+        first = srv.results()
+        srv.tick()
+        second = srv.results()
+    assert [r["id"] for r in first] == [2] and [r["id"] for r in second] == [1]
