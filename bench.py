@@ -41,7 +41,24 @@ WORKLOADS = {
     "incremental": {"total": 1 << 32, "step": 1 << 28, "source": 2, "seed": 11, "length": 6, "mode": "suffix"},
     "multi": {"total": 1 << 34, "step": 1 << 30, "source": 0, "seed": 23, "length": 0, "mode": "mixed",
               "launches": 4},
+    "serving": {"total": 0, "step": 0, "source": 0, "seed": 31, "length": 0, "mode": "mixed", "jobs": 1000,
+                "rate": 50.0, "budget": 1 << 26, "iters_per_tick": 8},
 }
+
+
+def serving_jobs(n=1000, rate=50.0, seed=31):
+    """Poisson arrivals (exponential gaps, mean 1/rate s) from numpy.random.default_rng(seed);
+    pattern length uniform in 4..8 over the base64 alphabet; mode uniform over case-sensitive
+    contains, case-sensitive suffix and case-insensitive contains."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    t, out = 0.0, []
+    for _ in range(n):
+        t += float(rng.exponential(1.0 / rate))
+        length = int(rng.integers(4, 9))
+        text = "".join(ALPHABET[int(v)] for v in rng.integers(0, 64, length))
+        out.append((t, text, ("contains", "suffix", "contains_ci")[int(rng.integers(0, 3))]))
+    return out
 
 # the multi-pattern workload's regexes: DFAs of 6..57 states (mk_regex_compile), each matching
 # a random key with probability 2e-7 .. 1.4e-4 (exact, by propagating a uniform character
@@ -342,7 +359,8 @@ def workload_config(workload, ctx, step_candidates=None, steps=None):
             "keys_per_thread": info["keys_per_thread"],
             "block": info["block"],
             "grid": info["grid"],
-            "inversion_batch": info["keys_per_thread"] * info["block"] // 32,
+            # keys sharing one field inversion: a thread's batch times the compute warps pooled per lane
+            "inversion_batch": info["keys_per_iter"] // (info["grid"] * 32),
             "l2": ("no memory-resident inputs: each thread steps its own point, the 14 KB step tables "
                    "stay on chip" if workload == "incremental" else
                    "inputs larger than L2: random gathers from the comb table in HBM"),
@@ -362,6 +380,132 @@ def traffic_per_key(workload):
         return None
 
 
+def _pct(xs, q):
+    xs = sorted(xs)
+    if not xs:
+        return None
+    return xs[min(len(xs) - 1, int(math.ceil(q * len(xs))) - 1)]
+
+
+def run_serving(args):
+    """Continuous batching against one job at a time on the same GPU, same jobs, same keys."""
+    import meikey_b200 as mk
+    wl = WORKLOADS["serving"]
+    n_jobs = args.serve_jobs or wl["jobs"]
+    jobs = serving_jobs(n_jobs, wl["rate"], wl["seed"])
+
+    def needle(text, mode):
+        return mk.Needle.suffix(text) if mode == "suffix" else mk.Needle.contains(text, case_sensitive=mode == "contains")
+    needles = [needle(t, m) for _, t, m in jobs]
+    key = hashlib.sha256(wl["seed"].to_bytes(8, "little")).digest()
+    ctx = mk.Context(device=0, table_rows=args.rows, keys_per_thread=args.kpt, block=args.block, self_check=True,
+                     hit_capacity=1 << 22)
+    budget, iters = wl["budget"], wl["iters_per_tick"]
+    # warm-up: a few ticks of a throw-away server
+    with mk.Server(ctx, key, max_jobs=4, iters_per_tick=iters, budget=budget, first=1 << 60) as warm:
+        for k in range(3):
+            warm.submit(needles[k], k)
+        for _ in range(args.warmup):
+            warm.tick()
+    clocks = ClockSampler(0)
+    clocks.start()
+    # serving: arrivals in real time, one tick after another while anything is admitted or queued
+    res, done_at = {}, {}
+    ticks = 0
+    with mk.Server(ctx, key, max_jobs=128, iters_per_tick=iters, budget=budget, hit_capacity=1 << 21) as srv:
+        t0 = time.perf_counter()
+        i = 0
+        busy = False
+        deadline = jobs[-1][0] + 600.0
+        while len(res) < n_jobs:
+            now = time.perf_counter() - t0
+            if now > deadline:
+                raise RuntimeError(f"serving run did not finish: {len(res)} of {n_jobs} jobs")
+            while i < n_jobs and jobs[i][0] <= now:
+                srv.submit(needles[i], i)
+                i += 1
+                busy = True
+            if not busy:
+                if i >= n_jobs:
+                    raise RuntimeError(f"serving run lost jobs: {len(res)} of {n_jobs}")
+                time.sleep(max(0.0, min(jobs[i][0] - now, 0.01)))
+                continue
+            active, queued = srv.tick()
+            ticks += 1
+            t_done = time.perf_counter() - t0
+            for r in srv.results():
+                res[r["id"]] = r
+                done_at[r["id"]] = t_done
+            busy = active + queued > 0
+        serve_span = time.perf_counter() - t0
+        stream = srv.position
+    clk = clocks.stop()
+    # one job at a time: FIFO in arrival order, each job searched alone from its admission
+    # index with the same budget (so the keys must be the same)
+    base_res, base_done = {}, {}
+    limit = min(n_jobs, args.serve_baseline_jobs or n_jobs)
+    single = ctx.job(key, mk.SEED_CHACHA20, [needles[0]])  # one job, its needle replaced per request
+    t0 = time.perf_counter()
+    for k in range(limit):
+        arrival = jobs[k][0]
+        now = time.perf_counter() - t0
+        if now < arrival:
+            time.sleep(arrival - now)
+        single.update([needles[k]])
+        base_res[k] = single.search(first=res[k]["admit_index"], max_tries=budget, iters=iters)
+        base_done[k] = time.perf_counter() - t0
+    base_span = time.perf_counter() - t0
+    single.close()
+    ctx.close()
+    identical = sum(1 for k in range(limit)
+                    if base_res[k]["found"] == res[k]["found"]
+                    and (not res[k]["found"] or (base_res[k]["index"], base_res[k]["pk"]) == (res[k]["index"], res[k]["pk"])))
+    ttk = [done_at[k] - jobs[k][0] for k in range(n_jobs) if res[k]["found"]]
+    ttk_all = [done_at[k] - jobs[k][0] for k in range(n_jobs)]
+    b_ttk = [base_done[k] - jobs[k][0] for k in range(limit) if base_res[k]["found"]]
+    b_all = [base_done[k] - jobs[k][0] for k in range(limit)]
+    tries = sum(r["tries"] for r in res.values())
+    b_tries = sum(base_res[k]["tries"] for k in range(limit))
+    value = tries / serve_span
+    b_value = b_tries / base_span
+    line = {
+        "metric": METRIC, "value": value, "unit": "keys/s", "n_gpus": 1, "steps": ticks, "warmup": args.warmup,
+        "ms_per_step": 1000 * serve_span / max(1, ticks), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": {
+            "workload": f"serving: {n_jobs} vanity jobs, Poisson arrivals at {wl['rate']:g}/s (numpy default_rng(31)), "
+                        "pattern length U{4..8}, mode uniform over case-sensitive contains / suffix / case-insensitive "
+                        "contains; continuous batching over one ChaCha20 candidate stream (key SHA-256(u64 31)), "
+                        f"per-job budget {budget} candidates, admission shortest-expected-first by needle slots "
+                        "and hit-ring plan",
+            "value_is": "aggregate job-keys/s: candidates searched for each job, summed over jobs, per second of the "
+                        "serving run (one candidate tested for n admitted jobs counts n times)",
+            "iters_per_tick": iters, "max_jobs": 128, "budget": budget,
+        },
+        "clocks": clk,
+        "gpu_launches": ticks,
+        "serving": {
+            "jobs": n_jobs, "found": len(ttk), "censored": n_jobs - len(ttk),
+            "p50_time_to_key_s": _pct(ttk, 0.5), "p99_time_to_key_s": _pct(ttk, 0.99),
+            "p50_time_to_result_s": _pct(ttk_all, 0.5), "p99_time_to_result_s": _pct(ttk_all, 0.99),
+            "jobs_per_s": n_jobs / serve_span, "span_s": serve_span,
+            "stream_candidates_per_s": stream / serve_span,
+        },
+        "one_at_a_time": {
+            "jobs": limit, "value": b_value, "unit": "keys/s", "found": len(b_ttk),
+            "p50_time_to_key_s": _pct(b_ttk, 0.5), "p99_time_to_key_s": _pct(b_ttk, 0.99),
+            "p50_time_to_result_s": _pct(b_all, 0.5), "p99_time_to_result_s": _pct(b_all, 0.99),
+            "jobs_per_s": limit / base_span, "span_s": base_span,
+        },
+        "identical_results": f"{identical}/{limit}",
+        "speedup_keys_per_s": value / b_value if b_value else None,
+        "speedup_jobs_per_s": (n_jobs / serve_span) / (limit / base_span),
+        "e2e": {"value": value, "unit": "keys/s", "note": "host wall clock around submit/tick/results, the public API"},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_ours(args):
     world, rank, local = dist_env()
     dist = Dist(world, local)
@@ -370,7 +514,8 @@ def run_ours(args):
     key, needle, source = workload_key(args.workload), workload_needle(args.workload), wl["source"]
     # the multi-pattern workload's 3-character patterns alone give ~1e-3 candidates per key
     ctx = mk.Context(device=local, table_rows=args.rows, keys_per_thread=args.kpt, block=args.block,
-                     self_check=True, hit_capacity=(1 << 22) if args.workload == "multi" else 0)
+                     self_check=True, hit_capacity=(1 << 22) if args.workload == "multi" else 0,
+                     hash_warps=args.hash_warps if source != 2 else 0)
     kpi = ctx.keys_per_iter
     launches = wl.get("launches", 1)  # > 1: a step is one replay of a CUDA graph of that many launches
     iters = math.ceil((args.step_candidates or wl["step"]) / (kpi * launches))
@@ -424,15 +569,10 @@ def run_ours(args):
                     g.launch(e2e_base)
             else:
                 j.launch(e2e_base, iters)
-            hits, total = j.hits(cap=1 << 22)
-            found += total
-            # one key per needle is written: confirm each needle's candidates in index order
-            # until one matches with its real x sign
-            done = set()
-            for index, nd in hits:
-                if nd not in done and j.confirm(index, nd)[0]:
-                    done.add(nd)
-            confirmed += len(done)
+            # one key per needle is written: each needle's candidates are confirmed on the host
+            # in index order until one matches with its real x sign (mk_job_first_matches)
+            found += j.hits(cap=0)[1]
+            confirmed += sum(m is not None for m in j.first_matches())
             a, b = j.io_bytes()
             h2d += a
             d2h += b
@@ -460,6 +600,7 @@ def run_ours(args):
         }
         cfg = workload_config(args.workload, ctx, step_keys, args.steps)
         cfg["launches_per_step"] = launches
+        cfg["hash_warps"] = args.hash_warps if source != 2 else 0
         cfg["needles"] = len(needles)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -493,8 +634,13 @@ def main():
     ap.add_argument("--rows", type=int, default=12, help="comb table rows")
     ap.add_argument("--kpt", type=int, default=16, help="keys per thread")
     ap.add_argument("--block", type=int, default=512)
+    ap.add_argument("--hash-warps", type=int, default=0, choices=[0, 4],
+                    help="4: search kernel with hashing warps (secure and multi workloads)")
     ap.add_argument("--e2e-steps", type=int, default=0, help="end-to-end steps (default: --steps)")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="secure")
+    ap.add_argument("--serve-jobs", type=int, default=0, help="serving: number of jobs (default 1000)")
+    ap.add_argument("--serve-baseline-jobs", type=int, default=0,
+                    help="serving: jobs run one at a time for the comparison (default: all)")
     ap.add_argument("--step-candidates", type=int, default=0,
                     help="candidates per step (default 2^30 secure, 2^28 incremental; smaller only for "
                          "profiling captures)")
@@ -504,6 +650,8 @@ def main():
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "serving":
+        return run_serving(args)
     return run_ours(args)
 
 

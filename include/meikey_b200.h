@@ -73,6 +73,9 @@ typedef struct mk_options {
     uint32_t blocks_per_sm;   /* resident CTAs per SM the grid is sized for (0 = occupancy maximum) */
     uint32_t self_check;      /* 1: derive keys at creation and compare with the host derivation */
     uint32_t hit_capacity;    /* hit-ring entries per job (0 = 65536) */
+    uint32_t hash_warps;      /* 4: search with hashing warps (block 512, keys per thread 8 or 16): 11 comb
+                                 warps, 1 inverter, 4 warps computing the SHA-512 scalars, so that hashing
+                                 overlaps the comb multiplies; ChaCha20 and counter seeds only.  0: off */
 } mk_options;
 
 /* One pattern as the reference's GPU needle (Needle, src/service/gpu.rs:618-660):
@@ -104,7 +107,7 @@ typedef struct mk_info {
     uint32_t keys_per_thread;
     uint32_t table_rows;
     uint64_t table_bytes;
-    uint64_t keys_per_iter;   /* grid · (block - 32) · keys_per_thread */
+    uint64_t keys_per_iter;   /* grid · (block - 32, or 352 with hash_warps) · keys_per_thread */
     char name[96];
 } mk_info;
 
@@ -214,6 +217,11 @@ MK_API int mk_graph_launch(mk_graph* graph, uint64_t base, int* found, uint64_t*
 MK_API int mk_graph_enqueue(mk_graph* graph, uint64_t base);
 MK_API void mk_graph_destroy(mk_graph* graph);
 
+/* For each needle k < n: the lowest candidate of the last launch (or graph replay) that the
+ * host confirms (mk_job_confirm, in index order), in out[k] (status MK_OK with index, key and
+ * secret; MK_ERR_STOPPED when none of its candidates matches with the real x sign). */
+MK_API int mk_job_first_matches(mk_job* job, mk_outcome* out, uint32_t n);
+
 /* Validates needles as mk_job_prepare would (host only, no device). */
 MK_API int mk_needles_check(const mk_needle* needles, uint32_t n_needles);
 /* keys_per_iter of the job's context */
@@ -311,6 +319,17 @@ MK_API int mk_autotune(int device, mk_tune_entry* entries, uint32_t n, uint32_t 
  * independent chains per thread at full occupancy: the measurement behind the choice of
  * limb radix (the search kernel is built for radix 2^32 only). */
 MK_API int mk_measure_field_mul(mk_ctx* ctx, double* radix32_per_s, double* radix26_per_s);
+
+/* OpenSSH output of a found key.  mk_openssh_public writes the authorized_keys line
+ * "ssh-ed25519 <base64 blob>[ comment]" (VanityKey::public_openssh, src/model/key.rs:132-139);
+ * mk_openssh_private writes the unencrypted openssh-key-v1 private key file of a seed
+ * (private_openssh, src/repository/key_file.rs:276-320; checkint is the file's random check
+ * word, a parameter so that tests can fix it).  Both write a NUL-terminated string, set
+ * *written to its length (without the NUL) and return MK_ERR_BAD_ARG when `cap` is too small
+ * or the comment holds a line break.  Host only; the private writer wipes its buffers. */
+MK_API int mk_openssh_public(const uint8_t pk[32], const char* comment, char* out, size_t cap, size_t* written);
+MK_API int mk_openssh_private(const uint8_t seed[32], const char* comment, uint32_t checkint, char* out, size_t cap,
+                              size_t* written);
 
 /* Comb table entry (row, column) as 24 words (y+x, y-x, 2dxy; row 0 holds 2xy), for tests. */
 MK_API int mk_table_entry(mk_ctx* ctx, uint32_t row, uint64_t col, uint32_t out[24]);

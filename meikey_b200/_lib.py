@@ -47,6 +47,7 @@ class Options(ctypes.Structure):
         ("blocks_per_sm", ctypes.c_uint32),
         ("self_check", ctypes.c_uint32),
         ("hit_capacity", ctypes.c_uint32),
+        ("hash_warps", ctypes.c_uint32),
     ]
 
 
@@ -152,6 +153,7 @@ SIGNATURES = [
                                    ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint32)]),
     ("mk_measure_field_mul", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
                                             ctypes.POINTER(ctypes.c_double)]),
+    ("mk_job_first_matches", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(OutcomeC), ctypes.c_uint32]),
     ("mk_needles_check", ctypes.c_int, [ctypes.POINTER(NeedleC), ctypes.c_uint32]),
     ("mk_job_keys_per_iter", ctypes.c_uint64, [ctypes.c_void_p]),
     ("mk_expected_tries", ctypes.c_double, [ctypes.POINTER(NeedleC)]),
@@ -165,6 +167,10 @@ SIGNATURES = [
                                          ctypes.POINTER(ctypes.c_uint32)]),
     ("mk_server_position", ctypes.c_uint64, [ctypes.c_void_p]),
     ("mk_server_destroy", None, [ctypes.c_void_p]),
+    ("mk_openssh_public", ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, ctypes.c_size_t,
+                                         ctypes.POINTER(ctypes.c_size_t)]),
+    ("mk_openssh_private", ctypes.c_int, [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_uint32, ctypes.c_char_p,
+                                          ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t)]),
     ("mk_derive_noalloc", ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_uint64,
                                          ctypes.c_uint64, ctypes.c_void_p]),
 ]

@@ -29,6 +29,7 @@ struct mk_ctx {
     uint4* incr = nullptr;           // incremental source: window table then step table
     uint32_t delta[24] = {};         // keys_per_iter·B (table form)
     uint32_t kpt = 8, block = 256, grid = 0;
+    uint32_t hash_warps = 0;  // 4: search kernel with hashing warps (ChaCha20 / counter seeds)
     uint32_t hit_capacity = 1u << 16;
     std::string err;
 };
@@ -203,7 +204,9 @@ int mk_ctx_create(int device, const mk_options* options, mk_ctx** out) {
     if (!o.block) o.block = 512;
     const bool built = (o.block == 256 && (o.keys_per_thread == 4 || o.keys_per_thread == 8 || o.keys_per_thread == 16)) ||
                        (o.block == 512 && (o.keys_per_thread == 8 || o.keys_per_thread == 16));
-    if (o.table_rows < 10 || o.table_rows > (uint32_t)mkb::MAX_ROWS || !built || o.blocks_per_sm > 16 || o.hit_capacity > (1u << 26))
+    const bool hw_ok = o.hash_warps == 0 || (o.hash_warps == 4 && o.block == 512 && (o.keys_per_thread == 8 || o.keys_per_thread == 16));
+    if (o.table_rows < 10 || o.table_rows > (uint32_t)mkb::MAX_ROWS || !built || !hw_ok || o.blocks_per_sm > 16 ||
+        o.hit_capacity > (1u << 26))
         return MK_ERR_OUT_OF_RANGE;
     mk_ctx* c = new (std::nothrow) mk_ctx;
     if (!c) return MK_ERR_OUT_OF_MEMORY;
@@ -211,6 +214,7 @@ int mk_ctx_create(int device, const mk_options* options, mk_ctx** out) {
     c->device = device;
     c->kpt = o.keys_per_thread;
     c->block = o.block;
+    c->hash_warps = o.hash_warps;
     if (o.hit_capacity) c->hit_capacity = o.hit_capacity;
     MK_CUDA(c, cudaSetDevice(device));
     MK_CUDA(c, cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
@@ -218,7 +222,7 @@ int mk_ctx_create(int device, const mk_options* options, mk_ctx** out) {
     cudaDeviceProp prop;
     MK_CUDA(c, cudaGetDeviceProperties(&prop, device));
     int occ = 0;
-    MK_CUDA(c, mkb::keys_occupancy(false, false, c->kpt, c->block, &occ));
+    MK_CUDA(c, mkb::keys_occupancy(false, false, c->kpt, c->block, c->hash_warps, &occ));
     if (occ < 1) return fail(c, MK_ERR_NOT_BUILT, "kernel does not fit on this device");
     uint32_t per_sm = o.blocks_per_sm ? std::min<uint32_t>(o.blocks_per_sm, (uint32_t)occ) : (uint32_t)occ;
     c->grid = (uint32_t)prop.multiProcessorCount * per_sm;
@@ -255,7 +259,7 @@ int mk_ctx_create(int device, const mk_options* options, mk_ctx** out) {
             return fail(c, MK_ERR_OUT_OF_MEMORY, "incremental table allocation failed");
         }
         MK_CUDA(c, cudaMemcpy(c->incr, words.data(), words.size() * 4, cudaMemcpyHostToDevice));
-        mkh25519::niels_of_multiple((uint64_t)c->grid * (c->block - 32) * c->kpt, c->delta);
+        mkh25519::niels_of_multiple((uint64_t)c->grid * mkb::search_threads(c->block, c->hash_warps) * c->kpt, c->delta);
     }
     // info
     mk_info& in = c->info;
@@ -267,7 +271,7 @@ int mk_ctx_create(int device, const mk_options* options, mk_ctx** out) {
     in.table_rows = c->geom.rows;
     in.table_bytes = bytes;
     // the search kernel's last warp per CTA inverts; the others derive keys
-    in.keys_per_iter = (uint64_t)c->grid * (c->block - 32) * c->kpt;
+    in.keys_per_iter = (uint64_t)c->grid * mkb::search_threads(c->block, c->hash_warps) * c->kpt;
     snprintf(in.name, sizeof in.name, "%.95s", prop.name);
     if (o.self_check) {
         int st = self_check(c);
@@ -470,6 +474,8 @@ int mk_job_prepare(mk_ctx* c, const uint8_t key[32], int seed_source, const mk_n
                    int stop_on_hit, mk_job** out) {
     if (!c || !key || !out || (n_needles && !needles)) return fail(c, MK_ERR_BAD_ARG, "bad argument");
     if (int st = check_source(c, key, seed_source)) return st;
+    if (seed_source == MK_SEED_INCREMENTAL && c->hash_warps)
+        return fail(c, MK_ERR_NOT_BUILT, "the hashing-warp search layout serves hashed seed sources only");
     *out = nullptr;
     MK_CUDA(c, cudaSetDevice(c->device));
     std::unique_ptr<mkb::MatchSet> ms(new (std::nothrow) mkb::MatchSet);
@@ -533,6 +539,15 @@ void mk_job_destroy(mk_job* j) {
     delete j;
 }
 
+// Shared memory for the job's DFA tables when they fit (the kernel then reads them there).
+static uint32_t dfa_smem_bytes(const mk_job* j) {
+    if (j->ctx->hash_warps) return 0;  // the hashing-warp kernel's scalar ring takes that shared memory
+    uint64_t total = 0;
+    for (const auto& h : j->needles)
+        if (h.mode == MK_MODE_REGEX) total += ((uint64_t)h.len * 130 + 15) & ~15ull;
+    return total <= mkb::DFA_SMEM_MAX ? (uint32_t)total : 0;
+}
+
 // Kernel parameters of one search launch of a job.
 static mkb::KeyLaunch search_params(const mk_job* j, uint64_t base, uint32_t iters) {
     const mk_ctx* c = j->ctx;
@@ -551,6 +566,8 @@ static mkb::KeyLaunch search_params(const mk_job* j, uint64_t base, uint32_t ite
     L.job = j->d_job;
     L.sink = j->d_sink;
     if (j->source == MK_SEED_INCREMENTAL) set_incremental(c, j->key, base, L);
+    L.dfa_smem = dfa_smem_bytes(j);
+    L.hash_warps = c->hash_warps;
     return L;
 }
 
@@ -631,6 +648,29 @@ int mk_job_confirm(mk_job* j, uint64_t index, uint32_t needle, uint8_t pk[32], u
     return MK_OK;
 }
 
+int mk_job_first_matches(mk_job* j, mk_outcome* out, uint32_t n) {
+    if (!j || (n && !out)) return MK_ERR_BAD_ARG;
+    for (uint32_t k = 0; k < n; k++) {
+        memset(&out[k], 0, sizeof out[k]);
+        out[k].status = MK_ERR_STOPPED;
+        out[k].needle = k;
+    }
+    std::vector<char> done(n, 0);
+    for (const mk_hit& h : j->last) {  // sorted by index
+        if (h.needle >= n || done[h.needle]) continue;
+        mk_outcome& o = out[h.needle];
+        int ok = 0;
+        int st = mk_job_confirm(j, h.index, h.needle, o.pk, o.secret, &ok);
+        if (st != MK_OK) return st;
+        if (ok) {
+            o.status = MK_OK;
+            o.index = h.index;
+            done[h.needle] = 1;
+        }
+    }
+    return MK_OK;
+}
+
 int mk_job_io_bytes(const mk_job* j, uint64_t* h2d, uint64_t* d2h) {
     if (!j || !h2d || !d2h) return MK_ERR_BAD_ARG;
     *h2d = j->h2d;
@@ -645,7 +685,7 @@ int mk_ctx_work_per_key(const mk_ctx* c, int seed_source, double* field_muls, do
     // a squaring 28 cross products + 8 diagonal ones (72) + 16
     const double MUL = 144.0, SQ = 88.0;
     const double kpt = c->kpt, rows = c->geom.rows;
-    const double ct = c->block - 32.0, groups = ct / 32.0;
+    const double ct = mkb::search_threads(c->block, c->hash_warps), groups = ct / 32.0;
     // comb: row 0 is free, full additions cost 7 multiplications, the last one 3
     double comb = 7.0 * (rows - 2) + 3.0;
     // Montgomery batch inside a thread: a_j and the running product (2 each for j > 0),
@@ -706,7 +746,8 @@ int mk_job_graph_create(mk_job* j, uint32_t iters, uint32_t launches, mk_graph**
     if (e != cudaSuccess) return bail(e, "cudaGraphAddMemsetNode");
     const void* func = nullptr;
     size_t dyn = 0;
-    e = mkb::keys_kernel(false, j->source == MK_SEED_INCREMENTAL, c->kpt, c->block, &func, &dyn);
+    e = mkb::keys_kernel(false, j->source == MK_SEED_INCREMENTAL, c->kpt, c->block, c->hash_warps, dfa_smem_bytes(j),
+                         &func, &dyn);
     if (e != cudaSuccess) return bail(e, "keys_kernel");
     for (uint32_t i = 0; i < launches; i++) {
         g->params[i] = search_params(j, g->span * i, iters);
@@ -734,6 +775,9 @@ static int graph_enqueue(mk_graph* g, uint64_t base) {
     mk_job* j = g->job;
     mk_ctx* c = j->ctx;
     MK_CUDA(c, cudaSetDevice(c->device));
+    // the job's needles may have changed since the graph was made: size the DFA staging anew
+    MK_CUDA(c, mkb::keys_kernel(false, j->source == MK_SEED_INCREMENTAL, c->kpt, c->block, c->hash_warps, dfa_smem_bytes(j), &g->func,
+                                &g->dyn));
     for (size_t i = 0; i < g->nodes.size(); i++) {
         g->params[i] = search_params(j, base + g->span * i, g->iters);
         void* args[] = {&g->params[i]};

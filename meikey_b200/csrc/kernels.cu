@@ -242,22 +242,32 @@ __device__ __forceinline__ void match_key(const MatchSet& ms, const u32 pk[8], u
             }
         }
     }
-    for (u32 r = 0; r < ms.n_regex; r++) {
-        const uint8_t* t = ms.dfa[r];
-        auto next = [&](u32 s, u32 i) -> u32 {
-            u64 at = ((u64)s * 65u + i) * 2u;
-            return (u32)__ldg(t + at) | (u32)__ldg(t + at + 1) << 8;
-        };
-        u32 s = 1, alt = 1;
+    // regex needles: four DFA walks side by side, so that their table lookups (shared
+    // memory when the launch staged the tables there, else global) overlap
+    for (u32 r0 = 0; r0 < ms.n_regex; r0 += 4) {
+        const uint16_t* t[4];
+        u32 s[4], alt[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            t[q] = reinterpret_cast<const uint16_t*>(ms.dfa[r0 + q < ms.n_regex ? r0 + q : r0]);
+            s[q] = alt[q] = 1;
+        }
 #pragma unroll 1
         for (int pos = 1; pos < 44; pos++) {
-            u32 v = vals[pos];
-            if (pos == MK_SIGN_POS) alt = next(s, v | 2u);
-            else if (pos > MK_SIGN_POS) alt = next(alt, v);
-            s = next(s, v);
+            const u32 v = tail_value(pk, pos);
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                if (pos == MK_SIGN_POS) alt[q] = t[q][s[q] * 65u + (v | 2u)];
+                else if (pos > MK_SIGN_POS) alt[q] = t[q][alt[q] * 65u + v];
+                s[q] = t[q][s[q] * 65u + v];
+            }
         }
-        bool ok = s == 0 || next(s, 64) != 0 || alt == 0 || next(alt, 64) != 0;
-        if (ok) {
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const u32 r = r0 + q;
+            if (r >= ms.n_regex) break;
+            const bool ok = s[q] == 0 || t[q][s[q] * 65u + 64u] != 0 || alt[q] == 0 || t[q][alt[q] * 65u + 64u] != 0;
+            if (!ok) continue;
             u32 id = ms.regex_id[r];
             hit_words[id >> 6] |= 1ull << (id & 63);
         }
@@ -510,6 +520,30 @@ __global__ void __launch_bounds__(BLOCK, 512 / BLOCK) k_search(const KeyLaunch L
         if (tid == 0) stop_iter = L.iters;
     }
     __syncthreads();
+    u32 dfa_need = 0;
+    for (u32 r = 0; r < ms.n_regex; r++) dfa_need += (ms.dfa_states[r] * 130u + 15u) & ~15u;
+    if (L.dfa_smem && dfa_need <= L.dfa_smem) {
+        // stage the job's DFA tables behind the other dynamic buffers (only when the launch
+        // reserved room for all of them) and point the matcher at the copies (16-byte
+        // aligned tables, copied in u16 units)
+        uint8_t* area = reinterpret_cast<uint8_t*>(INCR ? (void*)slots : (void*)(slots + CT));
+        u32 off = 0;
+        for (u32 r = 0; r < ms.n_regex; r++) {
+            const uint16_t* src = reinterpret_cast<const uint16_t*>(ms.dfa[r]);
+            uint16_t* dst = reinterpret_cast<uint16_t*>(area + off);
+            const u32 halves = ms.dfa_states[r] * 65u;
+            for (u32 i = tid; i < halves; i += BLOCK) dst[i] = src[i];
+            off += (halves * 2u + 15u) & ~15u;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            off = 0;
+            for (u32 r = 0; r < ms.n_regex; r++) {
+                ms.dfa[r] = area + off;
+                off += (ms.dfa_states[r] * 130u + 15u) & ~15u;
+            }
+        }
+    }
     if (tid == 0 && L.seed_src == 1) mid = mkh::counter_mid(key);
     __syncthreads();
     const u32 iters = L.iters;
@@ -565,6 +599,172 @@ __global__ void __launch_bounds__(BLOCK, 512 / BLOCK) k_search(const KeyLaunch L
         if (it + 1 < iters && it + 1 < stop_iter) produce(it + 1);
         bar_sync(3 + b, BLOCK);
         backward<KPT>(L, ms, first_of(it), batch[b], prod[b][tid], sink);
+        if (it + 1 >= iters || it + 1 >= stop_iter) break;
+    }
+    if (L.sink) L.sink[gid] = sink;
+}
+
+// Search kernel with hashing warps (ChaCha20 / counter seeds).  Warps 0..10 run the comb
+// multiplies, warp 11 inverts, warps 12..15 (one per SM sub-partition) compute the seeds'
+// SHA-512 scalars: hashing is ALU work and the comb is IMAD work, so the two pipes overlap
+// instead of the compute warps alternating between them.  The index layout and results are
+// those of k_search; only the division of work inside a CTA differs.
+//
+// Scalars go from the hashing warps to the comb warps through a two-slot shared ring of
+// chunks (4 keys of every comb thread per chunk).  Named barriers:
+//   1+b / 3+b  products / inverses of pipeline buffer b (comb warps and the inverter, 384)
+//   5+s / 7+s  ring slot s full / empty (hashing and comb warps, 480)
+//   9+(it&1)   the inverter's stop decision after iteration it (inverter and hashing warps, 160)
+// Whether iteration X is computed is decided, by every role, from the stop word as it stands
+// after the inverter's decision of iteration X-2; the inverter arrives on a decision barrier
+// only when the hashing warps will wait on it, and the hashing warps drain the last two ring
+// releases before they return, so no barrier phase is left open.
+template <int KPT, int BLOCK>
+__global__ void __launch_bounds__(BLOCK, 1) k_search_hw(const KeyLaunch L) {
+    static_assert(BLOCK == 512 && KPT % 4 == 0 && KPT >= 8, "layout of 11 comb, 1 inverter, 4 hashing warps");
+    constexpr int CW = 11, CT = CW * 32;     // comb warps / threads
+    constexpr int INV_WARP = 11;
+    constexpr int HT = 128;                  // hashing threads
+    constexpr int CPI = KPT / 4;             // ring chunks per iteration
+    constexpr int PAIRS = CT * 2;            // index pairs per chunk
+    constexpr int B_PIPE = CT + 32, B_RING = CT + HT, B_STOP = 32 + HT;
+    extern __shared__ uint4 dyn_smem[];
+    fe (*prod)[CT] = reinterpret_cast<fe (*)[CT]>(dyn_smem);
+    fe (*scratch)[CT] = prod + 2;
+    EntrySlot* slots = reinterpret_cast<EntrySlot*>(scratch + 2);
+    u64 (*ring)[4][CT][4] = reinterpret_cast<u64 (*)[4][CT][4]>(slots + CT);  // [slot][key][thread][word]
+    __shared__ CombGeom g;
+    __shared__ MatchSet ms;
+    __shared__ u32 key[8];
+    __shared__ mkh::CounterMid mid;
+    __shared__ volatile u32 stop_iter;
+    const u32 tid = threadIdx.x;
+    const u32 warp = tid >> 5;
+    {
+        const u32* src = (const u32*)&L.geom;
+        u32* dst = (u32*)&g;
+        for (u32 i = tid; i < sizeof(CombGeom) / 4; i += BLOCK) dst[i] = src[i];
+        const u32* s2 = (const u32*)L.match;
+        u32* d2 = (u32*)&ms;
+        for (u32 i = tid; i < sizeof(MatchSet) / 4; i += BLOCK) d2[i] = s2[i];
+        if (tid < 8) key[tid] = L.key[tid];
+        if (tid == 0) stop_iter = L.iters;
+    }
+    __syncthreads();
+    if (tid == 0 && L.seed_src == 1) mid = mkh::counter_mid(key);
+    __syncthreads();
+    const u32 iters = L.iters;
+    if (iters == 0) return;
+    const u64 nthreads = (u64)gridDim.x * CT;
+    auto first_of = [&](u32 it, u64 gid) { return L.base + ((u64)it * nthreads + gid) * KPT; };
+
+    if (warp > (u32)INV_WARP) {
+        // ---- hashing warps ----
+        const u32 p = tid - (INV_WARP + 1) * 32;
+        u32 X = 0;
+        for (;; X++) {
+            if (X >= iters) break;
+            if (X >= 2) {
+                bar_sync(9 + (X & 1), B_STOP);
+                if (X >= stop_iter) break;
+            }
+#pragma unroll 1
+            for (u32 c = 0; c < (u32)CPI; c++) {
+                const u32 gc = X * CPI + c, slot = gc & 1;
+                if (gc >= 2) bar_sync(7 + slot, B_RING);
+#pragma unroll 1
+                for (u32 v = p; v < (u32)PAIRS; v += HT) {
+                    const u32 t = v >> 1, k0 = (v & 1) * 2;
+                    const u64 idx = first_of(X, (u64)blockIdx.x * CT + t) + c * 4 + k0;
+                    u32 blk[16];
+                    u64 blk_id = ~0ull;
+#pragma unroll 1
+                    for (u32 q = 0; q < 2; q++) {
+                        u64 sc[4];
+                        scalar_of(L.seed_src, key, mid, idx + q, blk, blk_id, sc);
+                        uint4* d = reinterpret_cast<uint4*>(ring[slot][k0 + q][t]);
+                        d[0] = make_uint4((u32)sc[0], (u32)(sc[0] >> 32), (u32)sc[1], (u32)(sc[1] >> 32));
+                        d[1] = make_uint4((u32)sc[2], (u32)(sc[2] >> 32), (u32)sc[3], (u32)(sc[3] >> 32));
+                    }
+                }
+                bar_arrive(5 + slot, B_RING);
+            }
+        }
+        // the comb warps release every chunk they take: wait for the last two releases
+        const u32 G = X * CPI;
+        bar_sync(7 + ((G - 2) & 1), B_RING);
+        bar_sync(7 + ((G - 1) & 1), B_RING);
+        return;
+    }
+
+    if (warp == (u32)INV_WARP) {
+        // ---- inverter warp ----
+        for (u32 it = 0;; it++) {
+            const int b = it & 1;
+            bar_sync(1 + b, B_PIPE);
+            if ((tid & 31) == 0) {
+                const volatile JobDevice* jd = L.job;
+                if (jd->stop != 0 || (L.stop_on_hit && jd->hit_count != 0)) {
+                    u32 s = it + 2;
+                    if (s < stop_iter) stop_iter = s;
+                }
+            }
+            __syncwarp();
+            const bool more = it + 1 < iters && it + 1 < stop_iter;
+            // the hashing warps wait on this decision only when they will consider iteration it+2
+            if (it + 2 < iters && more) bar_arrive(9 + (it & 1), B_STOP);
+            invert_pools(prod[b], scratch[b], CW);
+            __syncwarp();
+            bar_arrive(3 + b, B_PIPE);
+            if (!more) break;
+        }
+        if ((tid & 31) == 0 && stop_iter < iters) atomicOr(&L.job->status, 1u);
+        return;
+    }
+
+    // ---- comb warps ----
+    const u64 gid = (u64)blockIdx.x * CT + tid;
+    EntrySlot& slot = slots[tid];
+    Batch<KPT> batch[2];
+    u32 sink = 0;
+    auto produce = [&](u32 it) {
+        const int b = it & 1;
+        Batch<KPT>& bt = batch[b];
+        fe run;
+#pragma unroll 1
+        for (int j = 0; j < KPT; j++) {
+            const u32 gc = it * CPI + (u32)(j >> 2), rs = gc & 1;
+            if ((j & 3) == 0) bar_sync(5 + rs, B_RING);
+            u64 sc[4];
+            {
+                const uint4* q = reinterpret_cast<const uint4*>(ring[rs][j & 3][tid]);
+                const uint4 a = q[0], c = q[1];
+                sc[0] = (u64)a.y << 32 | a.x;
+                sc[1] = (u64)a.w << 32 | a.z;
+                sc[2] = (u64)c.y << 32 | c.x;
+                sc[3] = (u64)c.w << 32 | c.z;
+            }
+            if ((j & 3) == 3) bar_arrive(7 + rs, B_RING);
+            fe num;
+            comb_mul(L.table, g, sc, slot, num, bt.den[j], nullptr, nullptr);
+            if (j == 0) {
+                bt.a[0] = num;
+                run = bt.den[0];
+            } else {
+                bt.a[j] = mk32::fe_mul(num, run);
+                run = mk32::fe_mul(run, bt.den[j]);
+            }
+        }
+        bt.prod = run;
+        prod[b][tid] = bt.prod;
+        bar_arrive(1 + b, B_PIPE);
+    };
+    produce(0);
+    for (u32 it = 0;; it++) {
+        const int b = it & 1;
+        if (it + 1 < iters && it + 1 < stop_iter) produce(it + 1);
+        bar_sync(3 + b, B_PIPE);
+        backward<KPT>(L, ms, first_of(it, gid), batch[b], prod[b][tid], sink);
         if (it + 1 >= iters || it + 1 >= stop_iter) break;
     }
     if (L.sink) L.sink[gid] = sink;
@@ -659,10 +859,21 @@ __global__ void __launch_bounds__(BLOCK, 512 / BLOCK) k_derive(const KeyLaunch L
 // dynamic shared memory: products and inversion scratch (two buffers each for the
 // search pipeline) and the per-thread table staging slots
 // (the incremental source reads no comb table and needs no staging slots)
-static size_t dyn_bytes(bool derive, bool incr, uint32_t block) {
+static size_t dyn_bytes(bool derive, bool incr, uint32_t block, uint32_t hw = 0) {
     const size_t fe_bytes = 32;
+    if (hw) {  // k_search_hw: 352 comb threads, plus the two-slot scalar ring of 4 keys each
+        const size_t ct = 352;
+        return 4 * ct * fe_bytes + ct * sizeof(EntrySlot) + 2 * 4 * ct * 32;
+    }
     const size_t threads = derive ? block : block - 32;  // the search kernel's last warp only inverts
     return (derive ? 2 : 4) * threads * fe_bytes + (incr ? 0 : threads * sizeof(EntrySlot));
+}
+
+static const void* hw_kernel_of(uint32_t kpt, uint32_t block) {
+    if (block != 512) return nullptr;
+    if (kpt == 8) return (const void*)k_search_hw<8, 512>;
+    if (kpt == 16) return (const void*)k_search_hw<16, 512>;
+    return nullptr;
 }
 
 static const void* kernel_of(bool derive, bool incr, uint32_t kpt, uint32_t block) {
@@ -683,27 +894,33 @@ static cudaError_t prepare(const void* f, size_t dyn) {
 cudaError_t launch_keys(const KeyLaunch& L, bool derive, uint32_t kpt, uint32_t block, uint32_t grid, cudaStream_t st) {
     const bool incr = L.seed_src == SEED_INCREMENTAL;
     if (incr && (kpt > (uint32_t)INCR_STEPS || !L.incr)) return cudaErrorInvalidValue;
-    const void* f = kernel_of(derive, incr, kpt, block);
+    if (L.dfa_smem > DFA_SMEM_MAX || (derive && L.dfa_smem)) return cudaErrorInvalidValue;
+    const bool hw = L.hash_warps && !derive && !incr;
+    if (hw && L.dfa_smem) return cudaErrorInvalidValue;  // the scalar ring takes that shared memory
+    const void* f = hw ? hw_kernel_of(kpt, block) : kernel_of(derive, incr, kpt, block);
     if (!f) return cudaErrorInvalidValue;
-    const size_t dyn = dyn_bytes(derive, incr, block);
+    const size_t dyn = dyn_bytes(derive, incr, block, hw ? 4 : 0) + L.dfa_smem;
     cudaError_t e = prepare(f, dyn);
     if (e != cudaSuccess) return e;
     void* args[] = {const_cast<KeyLaunch*>(&L)};
     return cudaLaunchKernel(f, dim3(grid), dim3(block), args, dyn, st);
 }
 
-cudaError_t keys_kernel(bool derive, bool incr, uint32_t kpt, uint32_t block, const void** func, size_t* dyn) {
-    const void* f = kernel_of(derive, incr, kpt, block);
-    if (!f) return cudaErrorInvalidValue;
+cudaError_t keys_kernel(bool derive, bool incr, uint32_t kpt, uint32_t block, uint32_t hash_warps, uint32_t dfa_smem,
+                        const void** func, size_t* dyn) {
+    const bool hw = hash_warps && !derive && !incr;
+    const void* f = hw ? hw_kernel_of(kpt, block) : kernel_of(derive, incr, kpt, block);
+    if (!f || dfa_smem > DFA_SMEM_MAX || (hw && dfa_smem)) return cudaErrorInvalidValue;
     *func = f;
-    *dyn = dyn_bytes(derive, incr, block);
+    *dyn = dyn_bytes(derive, incr, block, hw ? 4 : 0) + dfa_smem;
     return prepare(f, *dyn);
 }
 
-cudaError_t keys_occupancy(bool derive, bool incr, uint32_t kpt, uint32_t block, int* blocks_per_sm) {
-    const void* f = kernel_of(derive, incr, kpt, block);
+cudaError_t keys_occupancy(bool derive, bool incr, uint32_t kpt, uint32_t block, uint32_t hash_warps, int* blocks_per_sm) {
+    const bool hw = hash_warps && !derive && !incr;
+    const void* f = hw ? hw_kernel_of(kpt, block) : kernel_of(derive, incr, kpt, block);
     if (!f) return cudaErrorInvalidValue;
-    const size_t dyn = dyn_bytes(derive, incr, block);
+    const size_t dyn = dyn_bytes(derive, incr, block, hw ? 4 : 0);
     cudaError_t e = prepare(f, dyn);
     if (e != cudaSuccess) return e;
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, f, (int)block, dyn);

@@ -28,7 +28,17 @@ struct KeyLaunch {
     const uint4* incr;     // INCR_WINDOWS·16 entries j·16^w·B, then INCR_STEPS entries j·B (table form)
     uint32_t start[32];    // (s0 + base)·B as x, y, 1, xy
     uint32_t delta[24];    // keys_per_iter·B: one search thread's jump between iterations
+    // bytes of shared memory for the job's DFA tables (each 16-byte aligned; 0: read them
+    // from global memory)
+    uint32_t dfa_smem;
+    // 4: the search kernel with hashing warps (k_search_hw; ChaCha20 / counter seeds)
+    uint32_t hash_warps;
 };
+
+// compute threads of a search CTA: all but the inverter warp, or 11 comb warps with hashing warps
+inline uint32_t search_threads(uint32_t block, uint32_t hash_warps) { return hash_warps ? 352u : block - 32u; }
+
+constexpr uint32_t DFA_SMEM_MAX = 48u * 1024u;
 
 constexpr uint32_t SEED_INCREMENTAL = 2;
 constexpr int INCR_WINDOWS = 8;   // 4-bit windows of a thread's offset (offsets below 2^32)
@@ -40,8 +50,9 @@ cudaError_t launch_keys(const KeyLaunch& L, bool derive, uint32_t kpt, uint32_t 
 cudaError_t measure_field_mul_rates(int sms, cudaStream_t st, double* radix32_per_s, double* radix26_per_s);
 // The kernel of a variant and its dynamic shared memory (for graph nodes); sets the
 // kernel's shared-memory limit like launch_keys does.
-cudaError_t keys_kernel(bool derive, bool incr, uint32_t kpt, uint32_t block, const void** func, size_t* dyn);
-cudaError_t keys_occupancy(bool derive, bool incr, uint32_t kpt, uint32_t block, int* blocks_per_sm);
+cudaError_t keys_kernel(bool derive, bool incr, uint32_t kpt, uint32_t block, uint32_t hash_warps, uint32_t dfa_smem,
+                        const void** func, size_t* dyn);
+cudaError_t keys_occupancy(bool derive, bool incr, uint32_t kpt, uint32_t block, uint32_t hash_warps, int* blocks_per_sm);
 // multiply-adds per second of the carry-chain row microbenchmark and of plain mad.lo.u32
 cudaError_t measure_mad_peaks(int sms, cudaStream_t st, double* chain_per_s, double* lo_per_s);
 

@@ -101,13 +101,14 @@ extern "C" int mk_search(mk_job* job, const mk_search_config* cfg, mk_progress_f
     const double t0 = now_s();
     const uint64_t kpi = mk_job_keys_per_iter(job);
     if (kpi == 0) return MK_ERR_BAD_ARG;
-    const uint64_t end = cfg->max_tries ? cfg->first + cfg->max_tries : ~0ull;
+    // [first, end): at most max_tries indices, and never past the end of the 64-bit index space
+    const uint64_t end = (cfg->max_tries && cfg->max_tries <= ~0ull - cfg->first) ? cfg->first + cfg->max_tries : ~0ull;
     uint64_t base = cfg->first;
     std::vector<mk_hit> hits;
     for (;;) {
-        const uint64_t left = end - base;
-        const uint64_t want = (left + kpi - 1) / kpi;
-        const uint32_t iters = (uint32_t)std::min<uint64_t>(cfg->iters, want);
+        const uint64_t left = end - base;  // > 0 here
+        const uint64_t want = left / kpi + (left % kpi != 0);
+        const uint32_t iters = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(cfg->iters, want));
         int found = 0;
         uint64_t lowest = 0;
         int st = mk_job_launch(job, base, iters, &found, &lowest);
@@ -132,7 +133,8 @@ extern "C" int mk_search(mk_job* job, const mk_search_config* cfg, mk_progress_f
                 }
             }
         }
-        base += span;
+        const bool wrapped = base + span < base;
+        base = wrapped ? end : base + span;
         out->tries = std::min(base, end) - cfg->first;
         out->elapsed_s = now_s() - t0;
         if (base >= end) {
@@ -247,8 +249,8 @@ static int admit(mk_server* s) {
     for (auto it = s->queued.begin(); it != s->queued.end();) {
         if (s->active.size() >= s->opt.max_jobs) break;
         const double need = 4.0 * hits_per_tick(s, *it) + 64.0;
-        if (s->opt.hit_capacity && ring + need > s->opt.hit_capacity) {
-            ++it;  // waits until hit-ring memory frees up
+        if (s->opt.hit_capacity && ring + need > s->opt.hit_capacity && !s->active.empty()) {
+            ++it;  // waits until hit-ring memory frees up (a job is always admitted when none is active)
             continue;
         }
         // does it still fit the matcher's shift-and state / regex slots?

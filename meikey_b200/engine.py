@@ -77,9 +77,10 @@ class Context:
     """A device with the comb table built on it (Gpu::new / Kernel::load)."""
 
     def __init__(self, device: int = 0, table_rows: int = 12, keys_per_thread: int = 16, block: int = 512,
-                 blocks_per_sm: int = 0, self_check: bool = False, hit_capacity: int = 0):
+                 blocks_per_sm: int = 0, self_check: bool = False, hit_capacity: int = 0, hash_warps: int = 0):
         self._lib = L.load()
-        opts = L.Options(table_rows, keys_per_thread, block, blocks_per_sm, 1 if self_check else 0, hit_capacity)
+        opts = L.Options(table_rows, keys_per_thread, block, blocks_per_sm, 1 if self_check else 0, hit_capacity,
+                         hash_warps)
         ptr = ctypes.c_void_p()
         st = self._lib.mk_ctx_create(device, ctypes.byref(opts), ctypes.byref(ptr))
         self._ptr = ptr
@@ -240,6 +241,14 @@ class Job:
                 "tries": int(out.tries), "elapsed_s": float(out.elapsed_s), "secret": bytes(out.secret),
                 "pk": bytes(out.pk)}
 
+    def first_matches(self) -> List[Optional[dict]]:
+        """Per needle, the lowest host-confirmed key among the last launch's candidates, or None."""
+        n = len(self.needles)
+        out = (L.OutcomeC * max(1, n))()
+        _check(self._lib, self.ctx._ptr, self._lib.mk_job_first_matches(self._ptr, out, n))
+        return [{"index": int(out[k].index), "pk": bytes(out[k].pk), "secret": bytes(out[k].secret)}
+                if out[k].status == L.OK else None for k in range(n)]
+
     def confirm(self, index: int, needle: int):
         """Host confirmation of a candidate: (matched, public key, secret).  The secret is the
         seed (ChaCha20 / counter sources) or the scalar s0 + index (incremental source)."""
@@ -322,11 +331,13 @@ class Graph:
 BUILT_VARIANTS = [(4, 256), (8, 256), (16, 256), (8, 512), (16, 512)]
 
 
-def tune_space(rows=(11, 12, 13, 14, 16), variants=BUILT_VARIANTS, blocks_per_sm=(0,)):
+def tune_space(rows=(11, 12, 13, 14, 16), variants=BUILT_VARIANTS, blocks_per_sm=(0,), hash_warps=(0, 4)):
     """Candidate options: comb rows (table size against multiplications per key) x keys per
-    thread and block (inversion batch = keys per thread x compute warps) x CTAs per SM."""
-    return [dict(table_rows=r, keys_per_thread=k, block=b, blocks_per_sm=s)
-            for r in rows for (k, b) in variants for s in blocks_per_sm]
+    thread and block (inversion batch = keys per thread x compute warps) x CTAs per SM x the
+    hashing-warp layout (built for block 512, keys per thread 8 and 16)."""
+    return [dict(table_rows=r, keys_per_thread=k, block=b, blocks_per_sm=s, hash_warps=h)
+            for r in rows for (k, b) in variants for s in blocks_per_sm for h in hash_warps
+            if h == 0 or (b == 512 and k in (8, 16))]
 
 
 def autotune(device: int = 0, candidates=None, finalists: int = 3, trial_keys: int = 1 << 27):
@@ -335,7 +346,8 @@ def autotune(device: int = 0, candidates=None, finalists: int = 3, trial_keys: i
     cands = candidates or tune_space()
     arr = (L.TuneEntryC * len(cands))()
     for i, c in enumerate(cands):
-        arr[i].options = L.Options(c["table_rows"], c["keys_per_thread"], c["block"], c.get("blocks_per_sm", 0), 1, 0)
+        arr[i].options = L.Options(c["table_rows"], c["keys_per_thread"], c["block"], c.get("blocks_per_sm", 0), 1, 0,
+                                   c.get("hash_warps", 0))
     best = ctypes.c_uint32()
     st = lib.mk_autotune(device, arr, len(cands), finalists, trial_keys, ctypes.byref(best))
     if st != L.OK:
@@ -402,3 +414,25 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+def openssh_public(pk: bytes, comment: str = "") -> str:
+    """authorized_keys line of a public key (mk_openssh_public)."""
+    lib = L.load()
+    buf = ctypes.create_string_buffer(256 + 4 * len(comment.encode()))
+    n = ctypes.c_size_t()
+    st = lib.mk_openssh_public(bytes(pk), comment.encode(), buf, len(buf), ctypes.byref(n))
+    if st != L.OK:
+        raise GpuError(st, "openssh public line")
+    return buf.value.decode()
+
+
+def openssh_private(seed: bytes, comment: str = "", checkint: int = 0) -> str:
+    """Unencrypted openssh-key-v1 private key file of a seed (mk_openssh_private)."""
+    lib = L.load()
+    buf = ctypes.create_string_buffer(1024 + 4 * len(comment.encode()))
+    n = ctypes.c_size_t()
+    st = lib.mk_openssh_private(bytes(seed), comment.encode(), checkint, buf, len(buf), ctypes.byref(n))
+    if st != L.OK:
+        raise GpuError(st, "openssh private key")
+    return buf.value.decode()
