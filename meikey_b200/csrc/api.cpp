@@ -228,7 +228,7 @@ int mk_ctx_create(int device, const mk_options* options, mk_ctx** out) {
     c->grid = (uint32_t)prop.multiProcessorCount * per_sm;
     if (!make_geometry(o.table_rows, c->geom)) return fail(c, MK_ERR_OUT_OF_RANGE, "no comb geometry for this row count");
     // table
-    size_t bytes = (size_t)c->geom.entries * mkb::ENTRY_WORDS * 4;
+    size_t bytes = (size_t)c->geom.entries * mkb::COMB_STRIDE_WORDS * 4;
     e = cudaMalloc(&c->table, bytes);
     if (e != cudaSuccess) {
         c->table = nullptr;
@@ -375,7 +375,8 @@ int mk_derive_noalloc(mk_ctx* c, const uint8_t key[32], int seed_source, uint64_
 int mk_table_entry(mk_ctx* c, uint32_t row, uint64_t col, uint32_t out[24]) {
     if (!c || !out || row >= c->geom.rows || col >= c->geom.cols[row]) return fail(c, MK_ERR_BAD_ARG, "bad table entry");
     MK_CUDA(c, cudaSetDevice(c->device));
-    MK_CUDA(c, cudaMemcpy(out, c->table + (c->geom.row_base[row] + col) * (mkb::ENTRY_WORDS / 4), 96, cudaMemcpyDeviceToHost));
+    MK_CUDA(c, cudaMemcpy(out, c->table + (c->geom.row_base[row] + col) * (mkb::COMB_STRIDE_WORDS / 4), 96,
+                          cudaMemcpyDeviceToHost));
     return MK_OK;
 }
 

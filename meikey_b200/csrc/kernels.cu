@@ -97,9 +97,11 @@ __global__ void __launch_bounds__(256) k_build_table(uint4* table, const CombGeo
     mk32::fe_to_words(mk32::fe_add(y, x), w);
     mk32::fe_to_words(mk32::fe_sub(y, x), w + 8);
     mk32::fe_to_words(t, w + 16);
-    uint4* out = table + e * (ENTRY_WORDS / 4);
+    uint4* out = table + e * (COMB_STRIDE_WORDS / 4);
 #pragma unroll
     for (int q = 0; q < 6; q++) out[q] = make_uint4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
+#pragma unroll
+    for (int q = 6; q < COMB_STRIDE_WORDS / 4; q++) out[q] = make_uint4(0, 0, 0, 0);
 }
 
 // ---------------------------------------------------------------------------
@@ -113,7 +115,7 @@ struct EntrySlot {
 };
 
 __device__ __forceinline__ void fetch_entry(EntrySlot& slot, int which, const uint4* table, u64 idx) {
-    const uint4* src = table + idx * (ENTRY_WORDS / 4);
+    const uint4* src = table + idx * (COMB_STRIDE_WORDS / 4);
     u32 dst = (u32)__cvta_generic_to_shared(&slot.q[which][0]);
 #pragma unroll
     for (int q = 0; q < 6; q++)

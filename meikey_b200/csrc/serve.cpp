@@ -355,9 +355,12 @@ extern "C" int mk_server_tick(mk_server* s, uint32_t* active, uint32_t* queued) 
             closed[k] = 1;
         }
     }
-    size_t w = 0;
-    for (size_t k = 0; k < s->active.size(); k++)
-        if (!closed[k]) s->active[w++] = std::move(s->active[k]);
+    size_t w = 0;  // keep the open jobs in slot order (no self-move: it would empty the needle bytes)
+    for (size_t k = 0; k < s->active.size(); k++) {
+        if (closed[k]) continue;
+        if (w != k) s->active[w] = std::move(s->active[k]);
+        w++;
+    }
     if (w != s->active.size()) s->needles_dirty = true;
     s->active.resize(w);
     if (active) *active = (uint32_t)s->active.size();

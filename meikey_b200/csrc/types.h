@@ -24,6 +24,9 @@ struct CombGeom {
 
 // Words per table entry: (y+x, y-x, 2dxy) canonical, 8 little-endian u32 each.
 constexpr int ENTRY_WORDS = 24;
+// Comb-table entries sit 128 bytes apart (the last 32 bytes unused), so that every gather
+// reads exactly one aligned 128-byte line instead of straddling two half of the time.
+constexpr int COMB_STRIDE_WORDS = 32;
 
 // Matcher: up to MAX_NEEDLES needles tested in one pass.
 //   text needles (contains / suffix, fold): bit-parallel shift-and over the 43 searched

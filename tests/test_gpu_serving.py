@@ -111,3 +111,23 @@ def test_server_admits_shortest_expected_first(gpu_ctx):
         srv.tick()
         second = srv.results()
     assert [r["id"] for r in first] == [2] and [r["id"] for r in second] == [1]
+
+
+def test_server_keeps_open_jobs_when_a_later_slot_finishes(gpu_ctx):
+    """A long job in slot 0 stays open while a short job admitted after it (slot 1) finishes;
+    later ticks still carry the long job's needle and censor it at its budget."""
+    key = chacha_key(33)
+    kpi = gpu_ctx.keys_per_iter
+    long_job = mk.Needle.contains("Zq9xYw7")
+    short_job = mk.Needle.contains("ab", case_sensitive=False)
+    with mk.Server(gpu_ctx, key, max_jobs=4, iters_per_tick=1, budget=4 * kpi) as srv:
+        srv.submit(long_job, 1)
+        srv.tick()
+        assert srv.results() == []
+        srv.submit(short_job, 2)
+        srv.tick()
+        assert [r["id"] for r in srv.results()] == [2]
+        srv.tick()
+        srv.tick()
+        last = srv.results()
+    assert [(r["id"], r["found"], r["tries"]) for r in last] == [(1, False, 4 * kpi)]
