@@ -197,18 +197,29 @@ def dist_env():
     return world, rank, local
 
 
-class Dist:
-    """Barrier and max-over-ranks for the torchrun case (NCCL); no-ops for one process."""
+RANK_SHIFT = 56  # rank r searches indices r·2^56 ...: disjoint for any run shorter than 2^56 candidates
 
-    def __init__(self, world, local):
+
+def rank_first(rank: int, warmup: int, step_keys: int) -> int:
+    """First timed index of a rank: its own 2^56-wide range, after its warm-up steps."""
+    return (rank << RANK_SHIFT) + warmup * step_keys
+
+
+class Dist:
+    """Barrier and max-over-ranks for the torchrun case (NCCL on GPUs, gloo for CPU tests);
+    no-ops for one process.  The data path has no collective: ranks search disjoint ranges."""
+
+    def __init__(self, world, local, backend="nccl"):
         self.world = world
         self.pg = None
+        self.device = "cuda" if backend == "nccl" else "cpu"
         if world > 1:
             import datetime
             import torch
             import torch.distributed as dist
-            torch.cuda.set_device(local)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+            if backend == "nccl":
+                torch.cuda.set_device(local)
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
             self.torch, self.dist = torch, dist
             self.pg = True
 
@@ -219,7 +230,7 @@ class Dist:
     def max(self, x: float) -> float:
         if not self.pg:
             return x
-        t = self.torch.tensor([x], dtype=self.torch.float64, device="cuda")
+        t = self.torch.tensor([x], dtype=self.torch.float64, device=self.device)
         self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
         return float(t.item())
 
@@ -526,7 +537,7 @@ def run_ours(args):
     launches = wl.get("launches", 1)  # > 1: a step is one replay of a CUDA graph of that many launches
     iters = math.ceil((args.step_candidates or wl["step"]) / (kpi * launches))
     step_keys = kpi * iters * launches
-    rank_base = rank << 56
+    rank_base = rank_first(rank, 0, step_keys)
     peak, peak_lo = ctx.measure_mad_peaks()
     field_muls, mads_per_key = ctx.work_per_key(source)
     needles = workload_needles(args.workload)
@@ -548,7 +559,7 @@ def run_ours(args):
     dist.barrier()
     ctx.sync()
     ctx.record(0)
-    first = rank_base + args.warmup * step_keys
+    first = rank_first(rank, args.warmup, step_keys)
     for s in range(args.steps):
         enqueue_step(first + s * step_keys)
     ctx.record(1)
@@ -606,6 +617,7 @@ def run_ours(args):
         }
         cfg = workload_config(args.workload, ctx, step_keys, args.steps)
         cfg["launches_per_step"] = launches
+        cfg["options_from"] = "mk_autotune sweeps of rows x keys/thread x block (profiles/autotune_sweep.md)"
         cfg["hash_warps"] = args.hash_warps if source != 2 else 0
         cfg["needles"] = len(needles)
         line = {
@@ -642,7 +654,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--rows", type=int, default=12, help="comb table rows")
-    ap.add_argument("--kpt", type=int, default=16, help="keys per thread")
+    ap.add_argument("--kpt", type=int, default=8,
+                    help="keys per thread (8: the mk_autotune winner on B200, profiles/autotune_sweep.md)")
     ap.add_argument("--block", type=int, default=512)
     ap.add_argument("--hash-warps", type=int, default=0, choices=[0, 4],
                     help="4: search kernel with hashing warps (secure and multi workloads)")
