@@ -131,3 +131,19 @@ def test_server_keeps_open_jobs_when_a_later_slot_finishes(gpu_ctx):
         srv.tick()
         last = srv.results()
     assert [(r["id"], r["found"], r["tries"]) for r in last] == [(1, False, 4 * kpi)]
+
+
+def test_found_key_writes_openssh_files(gpu_ctx):
+    """End to end: mk_search finds and confirms a key, mk_openssh_* write it, the files load
+    in Python `cryptography` and the public line holds the pattern after the fixed prefix."""
+    from cryptography.hazmat.primitives import serialization
+    from meikey_b200.engine import openssh_private, openssh_public
+    key = chacha_key(34)
+    with gpu_ctx.job(key, mk.SEED_CHACHA20, [mk.Needle.contains("Q9z", case_sensitive=True)]) as job:
+        out = job.search(first=0, iters=4, time_limit_s=60)
+    assert out["found"]
+    pub = openssh_public(out["pk"], "vanity")
+    assert "Q9z" in pub.split()[1][25:]
+    priv = serialization.load_ssh_private_key(openssh_private(out["secret"], "vanity", 1).encode(), password=None)
+    raw = priv.public_key().public_bytes(serialization.Encoding.Raw, serialization.PublicFormat.Raw)
+    assert raw == out["pk"]
