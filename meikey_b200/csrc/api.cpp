@@ -311,6 +311,8 @@ static int check_source(mk_ctx* c, const uint8_t key[32], int seed_source) {
 int mk_derive(mk_ctx* c, const uint8_t key[32], int seed_source, uint64_t first, uint64_t n, uint8_t* out) {
     if (!c || !key || (!out && n)) return fail(c, MK_ERR_BAD_ARG, "bad argument");
     if (int st = check_source(c, key, seed_source)) return st;
+    if (seed_source == MK_SEED_INCREMENTAL && n > ~0ull - first + 1)
+        return fail(c, MK_ERR_OUT_OF_RANGE, "incremental indices must not wrap past 2^64");
     if (n == 0) return MK_OK;
     MK_CUDA(c, cudaSetDevice(c->device));
     const uint64_t per_launch = 1ull << 22;
@@ -574,6 +576,12 @@ static mkb::KeyLaunch search_params(const mk_job* j, uint64_t base, uint32_t ite
 
 static int enqueue(mk_job* j, uint64_t base, uint32_t iters) {
     mk_ctx* c = j->ctx;
+    // an incremental index is the scalar offset itself: a range that wraps past 2^64 would
+    // report indices whose keys are not the points the kernel stepped to
+    if (j->source == MK_SEED_INCREMENTAL) {
+        const unsigned __int128 end = (unsigned __int128)base + (unsigned __int128)c->info.keys_per_iter * iters;
+        if (end > ((unsigned __int128)1 << 64)) return fail(c, MK_ERR_OUT_OF_RANGE, "incremental indices must not wrap past 2^64");
+    }
     MK_CUDA(c, cudaSetDevice(c->device));
     MK_CUDA(c, cudaMemsetAsync(j->d_job, 0, 8, c->stream));  // hit_count and status; keep stop
     mkb::KeyLaunch L = search_params(j, base, iters);

@@ -433,3 +433,17 @@ def test_autotune_small_space():
 def test_field_mul_rates(gpu_ctx):
     r32, r26 = gpu_ctx.measure_field_mul()
     assert r32 > 1e10 and r26 > 1e10
+
+
+def test_incremental_range_must_not_wrap(gpu_ctx):
+    """Incremental indices are scalar offsets: ranges that would wrap past 2^64 are refused."""
+    s0 = _start_scalar(0)
+    kpi = gpu_ctx.keys_per_iter
+    with pytest.raises(mk.GpuError) as e:
+        gpu_ctx.derive(s0, mk.SEED_INCREMENTAL, 2**64 - 10, 11)
+    assert e.value.status == mk._lib.ERR_OUT_OF_RANGE
+    assert len(gpu_ctx.derive(s0, mk.SEED_INCREMENTAL, 2**64 - 10, 10)) == 320
+    with gpu_ctx.job(s0, mk.SEED_INCREMENTAL, [mk.Needle.contains("ab")]) as job:
+        with pytest.raises(mk.GpuError):
+            job.launch(2**64 - kpi + 1, 1)
+        job.launch(2**64 - kpi, 1)  # ends exactly at 2^64
