@@ -415,7 +415,7 @@ def run_serving(args):
         return mk.Needle.suffix(text) if mode == "suffix" else mk.Needle.contains(text, case_sensitive=mode == "contains")
     needles = [needle(t, m) for _, t, m in jobs]
     key = hashlib.sha256(wl["seed"].to_bytes(8, "little")).digest()
-    ctx = mk.Context(device=0, table_rows=args.rows, keys_per_thread=args.kpt, block=args.block, self_check=True,
+    ctx = mk.Context(device=0, table_rows=args.rows, keys_per_thread=args.kpt or 8, block=args.block, self_check=True,
                      hit_capacity=1 << 22)
     budget, iters = wl["budget"], wl["iters_per_tick"]
     # warm-up: a few ticks of a throw-away server
@@ -530,7 +530,8 @@ def run_ours(args):
     wl = WORKLOADS[args.workload]
     key, needle, source = workload_key(args.workload), workload_needle(args.workload), wl["source"]
     # the multi-pattern workload's 3-character patterns alone give ~1e-3 candidates per key
-    ctx = mk.Context(device=local, table_rows=args.rows, keys_per_thread=args.kpt, block=args.block,
+    kpt = args.kpt or (16 if source == 2 else 8)
+    ctx = mk.Context(device=local, table_rows=args.rows, keys_per_thread=kpt, block=args.block,
                      self_check=True, hit_capacity=(1 << 22) if args.workload == "multi" else 0,
                      hash_warps=args.hash_warps if source != 2 else 0)
     kpi = ctx.keys_per_iter
@@ -654,8 +655,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--rows", type=int, default=12, help="comb table rows")
-    ap.add_argument("--kpt", type=int, default=8,
-                    help="keys per thread (8: the mk_autotune winner on B200, profiles/autotune_sweep.md)")
+    ap.add_argument("--kpt", type=int, default=0,
+                    help="keys per thread (default: 8 for the hashed workloads, the mk_autotune winner on B200 in "
+                         "profiles/autotune_sweep.md; 16 for the incremental workload, whose per-iteration jump "
+                         "and inversion amortise over more keys)")
     ap.add_argument("--block", type=int, default=512)
     ap.add_argument("--hash-warps", type=int, default=0, choices=[0, 4],
                     help="4: search kernel with hashing warps (secure and multi workloads)")
