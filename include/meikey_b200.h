@@ -7,7 +7,10 @@
  * device.  All entry points return an `int` status (MK_OK = 0) and never abort the
  * process; the text of the last error of a context is kept in that context.
  * Plain pointers and sizes only: every buffer named "host" is ordinary host memory,
- * read or written only during the call.
+ * read or written only during the call.  A context, and the jobs, graphs and server made
+ * from it, are used from one host thread at a time (as the reference drives one Gpu per
+ * thread, src/service/search.rs:129-170); mk_job_stop is the exception and may be called
+ * from another thread while a launch of the job runs.
  *
  * Seeds (src/model/search.rs:27-50, src/service/gpu.rs:1330-1351):
  *   MK_SEED_CHACHA20  seed(i) = 32-byte half (i & 1) of ChaCha20 block i >> 1
@@ -217,6 +220,13 @@ MK_API int mk_graph_launch(mk_graph* graph, uint64_t base, int* found, uint64_t*
 MK_API int mk_graph_enqueue(mk_graph* graph, uint64_t base);
 MK_API void mk_graph_destroy(mk_graph* graph);
 
+/* Requests (on = 1) or withdraws (on = 0) a stop of the job's launches: the word is written
+ * from a separate stream, so it reaches a launch that is running; that launch ends within two
+ * iterations per CTA and reports MK_ERR_STOPPED, with the hits found until then.  The request
+ * stays set for later launches until withdrawn (the reference cancels between launches only,
+ * src/service/search.rs:33-40). */
+MK_API int mk_job_stop(mk_job* job, int on);
+
 /* For each needle k < n: the lowest candidate of the last launch (or graph replay) that the
  * host confirms (mk_job_confirm, in index order), in out[k] (status MK_OK with index, key and
  * secret; MK_ERR_STOPPED when none of its candidates matches with the real x sign). */
@@ -269,9 +279,11 @@ MK_API void mk_server_destroy(mk_server* server);
 MK_API int mk_job_confirm(mk_job* job, uint64_t index, uint32_t needle, uint8_t pk[32], uint8_t secret[32],
                           int* matched);
 
-/* Asynchronous form for timing: enqueue one launch on the context's stream without
- * waiting; mk_ctx_sync waits for all queued work. */
+/* Asynchronous form: enqueue one launch on the context's stream without waiting
+ * (mk_ctx_sync waits for all queued work); mk_job_collect waits and then reads the job word
+ * and hit ring like mk_job_launch does (hits of the last enqueued launch). */
 MK_API int mk_job_enqueue(mk_job* job, uint64_t base, uint32_t iters);
+MK_API int mk_job_collect(mk_job* job, int* found, uint64_t* index);
 MK_API int mk_ctx_sync(mk_ctx* ctx);
 /* CUDA events on the context's stream: record into slot (0..15); elapsed ms between two slots */
 MK_API int mk_ctx_record(mk_ctx* ctx, int slot);

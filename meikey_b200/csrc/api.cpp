@@ -22,6 +22,7 @@ using mkb::CombGeom;
 struct mk_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t side = nullptr;     // stop requests, written while a launch runs on `stream`
     cudaEvent_t ev[16] = {};
     mk_info info{};
     CombGeom geom{};
@@ -42,6 +43,7 @@ struct mk_job {
     std::vector<mkh25519::Needle> needles;
     mkb::MatchSet* d_match = nullptr;
     std::vector<uint8_t*> d_dfa;
+    uint32_t* d_gram4 = nullptr;  // 4-gram prefilter bitmap (2 MB), allocated on first use
     mkb::HitRecord* d_hits = nullptr;
     uint32_t cap = 1u << 16;
     mkb::JobDevice* d_job = nullptr;
@@ -218,6 +220,7 @@ int mk_ctx_create(int device, const mk_options* options, mk_ctx** out) {
     if (o.hit_capacity) c->hit_capacity = o.hit_capacity;
     MK_CUDA(c, cudaSetDevice(device));
     MK_CUDA(c, cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    MK_CUDA(c, cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
     for (auto& ev : c->ev) MK_CUDA(c, cudaEventCreate(&ev));
     cudaDeviceProp prop;
     MK_CUDA(c, cudaGetDeviceProperties(&prop, device));
@@ -288,6 +291,7 @@ void mk_ctx_destroy(mk_ctx* c) {
     if (c->incr) cudaFree(c->incr);
     for (auto& ev : c->ev)
         if (ev) cudaEventDestroy(ev);
+    if (c->side) cudaStreamDestroy(c->side);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
@@ -311,7 +315,7 @@ static int check_source(mk_ctx* c, const uint8_t key[32], int seed_source) {
 int mk_derive(mk_ctx* c, const uint8_t key[32], int seed_source, uint64_t first, uint64_t n, uint8_t* out) {
     if (!c || !key || (!out && n)) return fail(c, MK_ERR_BAD_ARG, "bad argument");
     if (int st = check_source(c, key, seed_source)) return st;
-    if (seed_source == MK_SEED_INCREMENTAL && n > ~0ull - first + 1)
+    if (seed_source == MK_SEED_INCREMENTAL && n != 0 && n - 1 > ~0ull - first)  // last index first + n - 1
         return fail(c, MK_ERR_OUT_OF_RANGE, "incremental indices must not wrap past 2^64");
     if (n == 0) return MK_OK;
     MK_CUDA(c, cudaSetDevice(c->device));
@@ -385,17 +389,22 @@ int mk_table_entry(mk_ctx* c, uint32_t row, uint64_t col, uint32_t out[24]) {
 // Compiles needles into a MatchSet on the host (src/service/gpu.rs:618-660 Needle::new,
 // dfa.rs:189-200): text needles become bit ranges of the shift-and state (a needle never
 // straddles a 64-bit word; fold lowercases the needle and accepts the uppercase value too),
-// DFA tables are validated and kept for upload.  No device work.
+// DFA tables are validated and kept for upload.  A job with GRAM4_MIN_NEEDLES or more text
+// needles of 4+ characters also gets the 4-gram prefilter: needles shorter than 4 are packed
+// first (the words every key scans), and `gram4` receives the bitmap of the long needles'
+// first 4-grams in every case variant.  No device work.
 static int pack_needles(mk_ctx* c, const mk_needle* needles, uint32_t n_needles, mkb::MatchSet& ms,
-                        std::vector<mkh25519::Needle>& hosts) {
+                        std::vector<mkh25519::Needle>& hosts, std::vector<uint32_t>* gram4) {
     if (n_needles && !needles) return fail(c, MK_ERR_BAD_ARG, "bad argument");
     if (n_needles > (uint32_t)mkb::MAX_NEEDLES) return fail(c, MK_ERR_BAD_ARG, "too many needles");
     memset(&ms, 0, sizeof ms);
     hosts.clear();
-    uint32_t bit = 0;  // next free bit in the shift-and state
+    hosts.resize(n_needles);
+    // validate and normalise every needle first
+    uint32_t long_text = 0;
     for (uint32_t i = 0; i < n_needles; i++) {
         const mk_needle& nd = needles[i];
-        mkh25519::Needle h;
+        mkh25519::Needle& h = hosts[i];
         h.mode = nd.mode;
         h.fold = nd.fold != 0;
         h.len = nd.len;
@@ -420,38 +429,96 @@ static int pack_needles(mk_ctx* c, const mk_needle* needles, uint32_t n_needles,
                 if (b64_value(ch) < 0) return fail(c, MK_ERR_PATTERN, "needle character outside the base64 alphabet");
                 if (h.fold && ch >= 'A' && ch <= 'Z') ch = (uint8_t)(ch + 32);
             }
-            if ((bit & 63) + nd.len > 64) bit = (bit + 63) & ~63u;
-            if (bit + nd.len > 64u * mkb::SA_WORDS) return fail(c, MK_ERR_BAD_ARG, "needles exceed the shift-and state");
-            for (uint32_t k = 0; k < nd.len; k++) {
-                uint32_t b = bit + k;
-                uint8_t ch = h.bytes[k];
-                int v = b64_value(ch);
-                ms.mask[v][b >> 6] |= 1ull << (b & 63);
-                if (h.fold && ch >= 'a' && ch <= 'z') ms.mask[v - 26][b >> 6] |= 1ull << (b & 63);
-            }
-            ms.first_bit[bit >> 6] |= 1ull << (bit & 63);
-            uint32_t last = bit + nd.len - 1;
-            if (nd.mode == MK_MODE_SUFFIX) ms.suffix_bit[last >> 6] |= 1ull << (last & 63);
-            else ms.last_bit[last >> 6] |= 1ull << (last & 63);
-            ms.text_id[ms.n_text] = (uint16_t)i;
-            ms.text_last[ms.n_text] = (uint16_t)last;
-            ms.n_text++;
-            bit += nd.len;
+            if (nd.len >= 4) long_text++;
         } else {
             return fail(c, MK_ERR_BAD_ARG, "unknown needle mode");
         }
-        hosts.push_back(std::move(h));
+    }
+    // the packing is the same whether or not the bitmap is wanted (gram4 null: check only)
+    const bool prefilter = long_text >= mkb::GRAM4_MIN_NEEDLES;
+    uint32_t bit = 0;  // next free bit in the shift-and state
+    auto place = [&](uint32_t i) -> int {
+        const mkh25519::Needle& h = hosts[i];
+        const uint32_t len = h.len;
+        if ((bit & 63) + len > 64) bit = (bit + 63) & ~63u;
+        if (bit + len > 64u * mkb::SA_WORDS) return fail(c, MK_ERR_BAD_ARG, "needles exceed the shift-and state");
+        for (uint32_t k = 0; k < len; k++) {
+            uint32_t b = bit + k;
+            uint8_t ch = h.bytes[k];
+            int v = b64_value(ch);
+            ms.mask[v][b >> 6] |= 1ull << (b & 63);
+            if (h.fold && ch >= 'a' && ch <= 'z') ms.mask[v - 26][b >> 6] |= 1ull << (b & 63);
+        }
+        ms.first_bit[bit >> 6] |= 1ull << (bit & 63);
+        uint32_t last = bit + len - 1;
+        if (h.mode == MK_MODE_SUFFIX) ms.suffix_bit[last >> 6] |= 1ull << (last & 63);
+        else ms.last_bit[last >> 6] |= 1ull << (last & 63);
+        ms.text_id[ms.n_text] = (uint16_t)i;
+        ms.text_last[ms.n_text] = (uint16_t)last;
+        ms.n_text++;
+        bit += len;
+        return MK_OK;
+    };
+    auto is_text = [&](uint32_t i) { return hosts[i].mode != MK_MODE_REGEX; };
+    if (prefilter) {
+        for (uint32_t i = 0; i < n_needles; i++)
+            if (is_text(i) && hosts[i].len < 4)
+                if (int st = place(i)) return st;
+        bit = (bit + 63) & ~63u;
+        ms.short_words = bit / 64;
+        for (uint32_t i = 0; i < n_needles; i++)
+            if (is_text(i) && hosts[i].len >= 4)
+                if (int st = place(i)) return st;
+        if (gram4) gram4->assign(mkb::GRAM4_WORDS, 0u);
+        for (uint32_t i = 0; gram4 && i < n_needles; i++) {
+            if (!is_text(i) || hosts[i].len < 4) continue;
+            const mkh25519::Needle& h = hosts[i];
+            // every case variant of the first four characters
+            int vals[4][2], nv[4];
+            for (int k = 0; k < 4; k++) {
+                const uint8_t ch = h.bytes[k];
+                vals[k][0] = b64_value(ch);
+                nv[k] = (h.fold && ch >= 'a' && ch <= 'z') ? 2 : 1;
+                vals[k][1] = vals[k][0] - 26;
+            }
+            for (int m = 0; m < 16; m++) {
+                bool ok = true;
+                uint32_t g = 0;
+                for (int k = 0; k < 4; k++) {
+                    const int pick = (m >> k) & 1;
+                    if (pick >= nv[k]) ok = false;
+                    g = g << 6 | (uint32_t)vals[k][pick];
+                }
+                if (ok) (*gram4)[g >> 5] |= 1u << (g & 31);
+            }
+        }
+    } else {
+        for (uint32_t i = 0; i < n_needles; i++)
+            if (is_text(i))
+                if (int st = place(i)) return st;
     }
     ms.sa_words = ms.n_text ? (bit + 63) / 64 : 0;
+    if (!prefilter) ms.short_words = ms.sa_words;
     return MK_OK;
 }
 
 // Uploads a packed MatchSet and its DFA tables to the job's device copy (after the job's
 // previous launches have finished).  DFA tables get fresh device buffers; text needles
 // need no allocation.
-static int upload_needles(mk_job* j, mkb::MatchSet& ms, std::vector<mkh25519::Needle>& hosts) {
+static int upload_needles(mk_job* j, mkb::MatchSet& ms, std::vector<mkh25519::Needle>& hosts,
+                          const std::vector<uint32_t>& gram4) {
     mk_ctx* c = j->ctx;
     MK_CUDA(c, cudaStreamSynchronize(c->stream));
+    ms.gram4 = nullptr;
+    if (!gram4.empty()) {
+        if (!j->d_gram4 && cudaMalloc(&j->d_gram4, gram4.size() * 4) != cudaSuccess) {
+            j->d_gram4 = nullptr;
+            return fail(c, MK_ERR_OUT_OF_MEMORY, "prefilter allocation");
+        }
+        MK_CUDA(c, cudaMemcpy(j->d_gram4, gram4.data(), gram4.size() * 4, cudaMemcpyHostToDevice));
+        j->h2d += gram4.size() * 4;
+        ms.gram4 = j->d_gram4;
+    }
     for (auto d : j->d_dfa) cudaFree(d);
     j->d_dfa.clear();
     for (uint32_t r = 0; r < ms.n_regex; r++) {
@@ -484,7 +551,8 @@ int mk_job_prepare(mk_ctx* c, const uint8_t key[32], int seed_source, const mk_n
     std::unique_ptr<mkb::MatchSet> ms(new (std::nothrow) mkb::MatchSet);
     if (!ms) return fail(c, MK_ERR_OUT_OF_MEMORY, "host allocation");
     std::vector<mkh25519::Needle> hosts;
-    if (int st = pack_needles(c, needles, n_needles, *ms, hosts)) return st;
+    std::vector<uint32_t> gram4;
+    if (int st = pack_needles(c, needles, n_needles, *ms, hosts, &gram4)) return st;
     mk_job* j = new (std::nothrow) mk_job;
     if (!j) return fail(c, MK_ERR_OUT_OF_MEMORY, "host allocation");
     j->ctx = c;
@@ -496,7 +564,7 @@ int mk_job_prepare(mk_ctx* c, const uint8_t key[32], int seed_source, const mk_n
         mk_job_destroy(j);
         return fail(c, code, msg);
     };
-    if (int st = upload_needles(j, *ms, hosts)) {
+    if (int st = upload_needles(j, *ms, hosts, gram4)) {
         std::string keep = c->err;
         mk_job_destroy(j);
         return fail(c, st, keep);
@@ -514,7 +582,7 @@ int mk_needles_check(const mk_needle* needles, uint32_t n_needles) {
     std::unique_ptr<mkb::MatchSet> ms(new (std::nothrow) mkb::MatchSet);
     if (!ms) return MK_ERR_OUT_OF_MEMORY;
     std::vector<mkh25519::Needle> hosts;
-    return pack_needles(nullptr, needles, n_needles, *ms, hosts);
+    return pack_needles(nullptr, needles, n_needles, *ms, hosts, nullptr);
 }
 
 uint64_t mk_job_keys_per_iter(const mk_job* j) { return j && j->ctx ? j->ctx->info.keys_per_iter : 0; }
@@ -526,8 +594,9 @@ int mk_job_update(mk_job* j, const mk_needle* needles, uint32_t n_needles) {
     std::unique_ptr<mkb::MatchSet> ms(new (std::nothrow) mkb::MatchSet);
     if (!ms) return fail(c, MK_ERR_OUT_OF_MEMORY, "host allocation");
     std::vector<mkh25519::Needle> hosts;
-    if (int st = pack_needles(c, needles, n_needles, *ms, hosts)) return st;
-    return upload_needles(j, *ms, hosts);
+    std::vector<uint32_t> gram4;
+    if (int st = pack_needles(c, needles, n_needles, *ms, hosts, &gram4)) return st;
+    return upload_needles(j, *ms, hosts, gram4);
 }
 
 void mk_job_destroy(mk_job* j) {
@@ -535,6 +604,7 @@ void mk_job_destroy(mk_job* j) {
     if (j->ctx) cudaSetDevice(j->ctx->device);
     if (j->ctx && j->ctx->stream) cudaStreamSynchronize(j->ctx->stream);
     for (auto d : j->d_dfa) cudaFree(d);
+    if (j->d_gram4) cudaFree(j->d_gram4);
     if (j->d_match) cudaFree(j->d_match);
     if (j->d_hits) cudaFree(j->d_hits);
     if (j->d_job) cudaFree(j->d_job);
@@ -621,6 +691,15 @@ static int collect(mk_job* j, int* found, uint64_t* index) {
     return MK_OK;
 }
 
+int mk_job_collect(mk_job* j, int* found, uint64_t* index) {
+    if (!j) return MK_ERR_BAD_ARG;
+    j->last.clear();
+    j->last_total = 0;
+    if (found) *found = 0;
+    MK_CUDA(j->ctx, cudaSetDevice(j->ctx->device));
+    return collect(j, found, index);
+}
+
 int mk_job_launch(mk_job* j, uint64_t base, uint32_t iters, int* found, uint64_t* index) {
     if (!j) return MK_ERR_BAD_ARG;
     j->last.clear();
@@ -654,6 +733,17 @@ int mk_job_confirm(mk_job* j, uint64_t index, uint32_t needle, uint8_t pk[32], u
         mkh25519::public_key(secret, pk);
     }
     *matched = mkh25519::matches(j->needles[needle], pk) ? 1 : 0;
+    return MK_OK;
+}
+
+int mk_job_stop(mk_job* j, int on) {
+    if (!j) return MK_ERR_BAD_ARG;
+    mk_ctx* c = j->ctx;
+    MK_CUDA(c, cudaSetDevice(c->device));
+    // the job word's stop field (nonzero = stop), set on the side stream so that it lands
+    // while a launch of this job runs on the context's stream
+    MK_CUDA(c, cudaMemsetAsync(&j->d_job->stop, on ? 1 : 0, sizeof(uint32_t), c->side));
+    MK_CUDA(c, cudaStreamSynchronize(c->side));
     return MK_OK;
 }
 

@@ -221,8 +221,24 @@ __device__ __forceinline__ void match_key(const MatchSet& ms, const u32 pk[8], u
     u32 vals[44];
 #pragma unroll
     for (int pos = 1; pos < 44; pos++) vals[pos] = tail_value(pk, pos);
-    // text needles: shift-and over sa_words words of state
-    for (u32 wi = 0; wi < ms.sa_words; wi++) {
+    // text needles: shift-and over sa_words words of state.  With the 4-gram prefilter, the
+    // words of the needles of 4+ characters are scanned only when one of the key's 4-character
+    // windows (position 42 with both values) is the start of such a needle.
+    u32 words = ms.sa_words;
+    if (ms.gram4) {
+        u32 any = 0, gw = vals[1] << 12 | vals[2] << 6 | vals[3];
+#pragma unroll
+        for (int p = 1; p + 3 < 44; p++) {
+            gw = (gw << 6 | vals[p + 3]) & 0xffffffu;
+            any |= __ldg(ms.gram4 + (gw >> 5)) >> (gw & 31);
+            if (p <= MK_SIGN_POS && MK_SIGN_POS <= p + 3) {
+                const u32 g2 = gw | 2u << (6 * (p + 3 - MK_SIGN_POS));
+                any |= __ldg(ms.gram4 + (g2 >> 5)) >> (g2 & 31);
+            }
+        }
+        if (!(any & 1u)) words = ms.short_words;
+    }
+    for (u32 wi = 0; wi < words; wi++) {
         u64 D = 0, acc = 0;
         u64 first = ms.first_bit[wi], last = ms.last_bit[wi];
 #pragma unroll

@@ -39,7 +39,8 @@ struct MatchSet {
     uint32_t n_text;              // text needles packed into the shift-and state
     uint32_t n_regex;             // regex needles
     uint32_t sa_words;            // words of shift-and state in use
-    uint32_t pad;
+    uint32_t short_words;         // with gram4: the leading words, holding the needles shorter than 4
+                                  // characters, that every key scans; the rest only when gram4 fires
     // shift-and: per value v (0..63) the bits of needle positions accepting v
     uint64_t mask[64][SA_WORDS];
     uint64_t first_bit[SA_WORDS]; // bit 0 of every text needle (set on each step)
@@ -51,7 +52,14 @@ struct MatchSet {
     const uint8_t* dfa[16];
     uint32_t dfa_states[16];
     uint16_t regex_id[16];
+    // prefilter of the text needles of 4 or more characters (null: none): bit g of 2^24 is set
+    // when some such needle starts with the 4 base64 values g = v0<<18 | v1<<12 | v2<<6 | v3
+    // (all case variants of a folded needle)
+    const uint32_t* gram4;
 };
+
+constexpr uint32_t GRAM4_WORDS = 1u << 19;  // 2^24 bits
+constexpr uint32_t GRAM4_MIN_NEEDLES = 8;   // long text needles from which a job uses the prefilter
 
 struct HitRecord {
     uint64_t index;

@@ -241,6 +241,19 @@ class Job:
                 "tries": int(out.tries), "elapsed_s": float(out.elapsed_s), "secret": bytes(out.secret),
                 "pk": bytes(out.pk)}
 
+    def stop(self, on: bool = True):
+        """Request (or withdraw) a stop of this job's launches, also of one that is running."""
+        _check(self._lib, self.ctx._ptr, self._lib.mk_job_stop(self._ptr, 1 if on else 0))
+
+    def collect(self) -> Optional[int]:
+        """Waits for the job's queued launches and reads their hits (like launch, without launching)."""
+        found = ctypes.c_int()
+        idx = ctypes.c_uint64()
+        st = self._lib.mk_job_collect(self._ptr, ctypes.byref(found), ctypes.byref(idx))
+        if st not in (L.OK, L.ERR_STOPPED, L.ERR_HIT_RING_FULL):
+            _check(self._lib, self.ctx._ptr, st)
+        return int(idx.value) if found.value else None
+
     def first_matches(self) -> List[Optional[dict]]:
         """Per needle, the lowest host-confirmed key among the last launch's candidates, or None."""
         n = len(self.needles)

@@ -447,3 +447,64 @@ def test_incremental_range_must_not_wrap(gpu_ctx):
         with pytest.raises(mk.GpuError):
             job.launch(2**64 - kpi + 1, 1)
         job.launch(2**64 - kpi, 1)  # ends exactly at 2^64
+
+
+def test_stop_request_ends_a_running_launch(gpu_ctx):
+    """mk_job_stop written while a long launch runs: the launch ends early with STOPPED and its
+    hits lie in the first iterations; after withdrawing the request a launch runs in full."""
+    import time
+    key = chacha_key(12)
+    kpi = gpu_ctx.keys_per_iter
+    with gpu_ctx.job(key, mk.SEED_CHACHA20, [mk.Needle.contains("Ab9")]) as job:
+        job.enqueue(0, 4096)  # several seconds of work
+        time.sleep(0.2)
+        job.stop(True)
+        t0 = time.perf_counter()
+        job.collect()
+        waited = time.perf_counter() - t0
+        hits, total = job.hits(cap=1 << 18)
+        assert waited < 2.0
+        assert hits and max(i for i, _ in hits) < 4096 * kpi // 4
+        job.stop(False)
+        job.launch(0, 2)
+        full, _ = job.hits(cap=1 << 18)
+    assert full and max(i for i, _ in full) >= kpi
+
+
+def test_prefilter_finds_needles_cut_from_keys(gpu_ctx, oracle):
+    """Jobs of 8+ long text needles use the 4-gram prefilter.  Needles cut from the text of
+    known keys (at offsets up to the end, across the sign-dependent position 42, some folded
+    or as suffixes) must report their source keys, and every needle's hits must equal the
+    oracle's candidates; two short needles ride along unfiltered."""
+    key = chacha_key(44)
+    base = 9_000_001
+    n = gpu_ctx.keys_per_iter
+    rng = random.Random(44)
+    needles, sources = [], []
+    for k in range(14):
+        idx = base + rng.randrange(n)
+        pk = bytearray(oracle.derive(key, 0, idx, 1))
+        pk[31] &= 0x7F  # the y-only key the GPU sees; position 42 is tried with both values
+        hay = oracle.public_b64(bytes(pk))[25:]
+        length = rng.randint(4, 8)
+        start = 42 - rng.randint(1, 3) if k % 3 == 0 else rng.randrange(0, 44 - length)
+        start = max(0, min(start, 43 - length))
+        text = hay[start:start + length]
+        if k % 4 == 1:
+            needles.append(mk.Needle.suffix(hay[43 - length:]))
+        elif k % 4 == 2:
+            needles.append(mk.Needle.contains(text.swapcase(), case_sensitive=False))
+        else:
+            needles.append(mk.Needle.contains(text))
+        sources.append(idx)
+    needles += [mk.Needle.contains("q9"), mk.Needle.suffix("Z")]
+    with gpu_ctx.job(key, mk.SEED_CHACHA20, needles) as job:
+        job.launch(base, 1)
+        hits, total = job.hits(cap=1 << 18)
+    assert total == len(hits)
+    pks = oracle.derive(key, 0, base, n)
+    for k, nd in enumerate(needles):
+        got = [i for i, j in hits if j == k]
+        assert got == oracle.match_keys(pks, base, nd.text, len(nd.text), nd.fold, nd.mode), k
+        if k < len(sources):
+            assert sources[k] in got, k
