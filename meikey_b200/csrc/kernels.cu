@@ -260,13 +260,13 @@ __device__ __forceinline__ void match_key(const MatchSet& ms, const u32 pk[8], u
             }
         }
     }
-    // regex needles: four DFA walks side by side, so that their table lookups (shared
+    // regex needles: eight DFA walks side by side, so that their table lookups (shared
     // memory when the launch staged the tables there, else global) overlap
-    for (u32 r0 = 0; r0 < ms.n_regex; r0 += 4) {
-        const uint16_t* t[4];
-        u32 s[4], alt[4];
+    for (u32 r0 = 0; r0 < ms.n_regex; r0 += 8) {
+        const uint16_t* t[8];
+        u32 s[8], alt[8];
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
+        for (int q = 0; q < 8; q++) {
             t[q] = reinterpret_cast<const uint16_t*>(ms.dfa[r0 + q < ms.n_regex ? r0 + q : r0]);
             s[q] = alt[q] = 1;
         }
@@ -274,14 +274,14 @@ __device__ __forceinline__ void match_key(const MatchSet& ms, const u32 pk[8], u
         for (int pos = 1; pos < 44; pos++) {
             const u32 v = tail_value(pk, pos);
 #pragma unroll
-            for (int q = 0; q < 4; q++) {
+            for (int q = 0; q < 8; q++) {
                 if (pos == MK_SIGN_POS) alt[q] = t[q][s[q] * 65u + (v | 2u)];
                 else if (pos > MK_SIGN_POS) alt[q] = t[q][alt[q] * 65u + v];
                 s[q] = t[q][s[q] * 65u + v];
             }
         }
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
+        for (int q = 0; q < 8; q++) {
             const u32 r = r0 + q;
             if (r >= ms.n_regex) break;
             const bool ok = s[q] == 0 || t[q][s[q] * 65u + 64u] != 0 || alt[q] == 0 || t[q][alt[q] * 65u + 64u] != 0;
