@@ -577,24 +577,39 @@ def run_ours(args):
     e2e_steps = args.e2e_steps or args.steps
     h2d = d2h = 0
     found = confirmed = 0
+    phases = {"prepare": 0.0, "launch_and_wait": 0.0, "read_hits": 0.0, "confirm": 0.0, "release": 0.0}
+    e2e_clocks = ClockSampler(local)
+    e2e_clocks.start()
     dist.barrier()
     t0 = time.perf_counter()
     for s in range(e2e_steps):
-        with ctx.job(key, source, workload_needles(args.workload)) as j:
-            e2e_base = first + (args.steps + s) * step_keys
-            if launches > 1:
-                with j.graph(iters, launches) as g:
-                    g.launch(e2e_base)
-            else:
-                j.launch(e2e_base, iters)
-            # one key per needle is written: each needle's candidates are confirmed on the host
-            # in index order until one matches with its real x sign (mk_job_first_matches)
-            found += j.hits(cap=0)[1]
-            confirmed += sum(m is not None for m in j.first_matches())
-            a, b = j.io_bytes()
-            h2d += a
-            d2h += b
+        tp = time.perf_counter()
+        j = ctx.job(key, source, workload_needles(args.workload))
+        g = j.graph(iters, launches) if launches > 1 else None
+        tl = time.perf_counter()
+        e2e_base = first + (args.steps + s) * step_keys
+        if g is not None:
+            g.launch(e2e_base)
+        else:
+            j.launch(e2e_base, iters)
+        tr = time.perf_counter()
+        found += j.hits(cap=0)[1]
+        tc = time.perf_counter()
+        # one key per needle is written: each needle's candidates are confirmed on the host
+        # in index order until one matches with its real x sign (mk_job_first_matches)
+        confirmed += sum(m is not None for m in j.first_matches())
+        a, b = j.io_bytes()
+        h2d += a
+        d2h += b
+        tx = time.perf_counter()
+        if g is not None:
+            g.close()
+        j.close()
+        te = time.perf_counter()
+        for name, (x, y) in zip(phases, ((tp, tl), (tl, tr), (tr, tc), (tc, tx), (tx, te))):
+            phases[name] += y - x
     dt_e2e = time.perf_counter() - t0
+    e2e_clk = e2e_clocks.stop()
     dt_e2e = dist.max(dt_e2e)
     e2e = step_keys * e2e_steps * world / dt_e2e
     if graph is not None:
@@ -628,7 +643,9 @@ def run_ours(args):
             "gpu_launches": args.steps * launches,
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d // e2e_steps,
                     "d2h_bytes_per_step": d2h // e2e_steps, "steps": e2e_steps, "candidates": found,
-                    "needles_confirmed_on_host": confirmed},
+                    "needles_confirmed_on_host": confirmed,
+                    "ms_per_step_by_phase": {k: round(1000 * v / e2e_steps, 3) for k, v in phases.items()},
+                    "clocks": e2e_clk},
             "roofline": roofline,
             "device": ctx_info["name"],
         }
