@@ -248,7 +248,10 @@ MK_API double mk_expected_tries(const mk_needle* needle);
  * that matches with its real x sign is returned: the lowest matching index of the range.
  * Stops with status MK_ERR_STOPPED when max_tries indices are searched, the time limit passes
  * or `progress` returns nonzero (checked between launches, so a cancel takes effect within
- * one launch).  The return value is an error of the engine, else MK_OK. */
+ * one launch).  A launch whose candidates overflow the job's hit ring is run again over the
+ * same start in launches of half the iterations; MK_ERR_HIT_RING_FULL is returned only when
+ * a single iteration overflows it (raise mk_options.hit_capacity).  The return value is an
+ * error of the engine, else MK_OK. */
 MK_API int mk_search(mk_job* job, const mk_search_config* cfg, mk_progress_fn progress, void* user,
                      mk_outcome* out);
 

@@ -108,10 +108,16 @@ extern "C" int mk_search(mk_job* job, const mk_search_config* cfg, mk_progress_f
     for (;;) {
         const uint64_t left = end - base;  // > 0 here
         const uint64_t want = left / kpi + (left % kpi != 0);
-        const uint32_t iters = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(cfg->iters, want));
+        uint32_t iters = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(cfg->iters, want));
         int found = 0;
         uint64_t lowest = 0;
         int st = mk_job_launch(job, base, iters, &found, &lowest);
+        // more candidates than the hit ring holds: the kept ones need not be the lowest, so
+        // the same range is searched again in shorter launches (down to one iteration)
+        while (st == MK_ERR_HIT_RING_FULL && iters > 1) {
+            iters /= 2;
+            st = mk_job_launch(job, base, iters, &found, &lowest);
+        }
         if (st != MK_OK && st != MK_ERR_STOPPED) return st;
         const uint64_t span = kpi * iters;
         if (found) {

@@ -147,3 +147,16 @@ def test_found_key_writes_openssh_files(gpu_ctx):
     priv = serialization.load_ssh_private_key(openssh_private(out["secret"], "vanity", 1).encode(), password=None)
     raw = priv.public_key().public_bytes(serialization.Encoding.Raw, serialization.PublicFormat.Raw)
     assert raw == out["pk"]
+
+
+def test_search_reruns_overflowing_launches(gpu_ctx, oracle):
+    """A launch of 16 iterations with a frequent needle overflows the hit ring (2^18 records);
+    mk_search searches the range again in shorter launches and still returns the lowest
+    confirmed key, the same as a search of one iteration per launch."""
+    key = chacha_key(35)
+    nd = mk.Needle.contains("ab", case_sensitive=False)  # about 4 % of keys are candidates
+    with gpu_ctx.job(key, mk.SEED_CHACHA20, [nd]) as job:
+        wide = job.search(first=7, iters=16)
+        narrow = job.search(first=7, iters=1)
+    assert wide["found"] and (wide["index"], wide["pk"]) == (narrow["index"], narrow["pk"])
+    assert _first_full_match(oracle, key, 0, 7, wide["index"], nd) == wide["index"]
