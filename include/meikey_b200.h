@@ -330,10 +330,14 @@ MK_API int mk_autotune(int device, mk_tune_entry* entries, uint32_t n, uint32_t 
                        uint32_t* best);
 
 /* Field multiplications per second on the context's device in radix 2^32 (the search
- * kernel's eight-limb field) and radix 2^25.5 (ten limbs, 100 mad.wide products), four
- * independent chains per thread at full occupancy: the measurement behind the choice of
- * limb radix (the search kernel is built for radix 2^32 only). */
-MK_API int mk_measure_field_mul(mk_ctx* ctx, double* radix32_per_s, double* radix26_per_s);
+ * kernel's eight-limb field), radix 2^25.5 (ten limbs, 100 mad.wide products) and radix
+ * 2^51 held in FP64 registers (five limbs, products split exactly by fused multiply-adds,
+ * the reference's F51 limbs, src/service/gpu/kernel.cu:1318-1441), four independent chains
+ * per thread at full occupancy: the measurement behind the choice of limb radix (the search
+ * kernel is built for radix 2^32 only).  The radix-2^51 chains are also run against radix
+ * 2^32 from the same inputs; MK_ERR_SELF_CHECK if any result differs. */
+MK_API int mk_measure_field_mul(mk_ctx* ctx, double* radix32_per_s, double* radix26_per_s,
+                                double* radix51_fp64_per_s);
 
 /* OpenSSH output of a found key.  mk_openssh_public writes the authorized_keys line
  * "ssh-ed25519 <base64 blob>[ comment]" (VanityKey::public_openssh, src/model/key.rs:132-139);

@@ -919,10 +919,13 @@ void mk_graph_destroy(mk_graph* g) {
     delete g;
 }
 
-int mk_measure_field_mul(mk_ctx* c, double* radix32_per_s, double* radix26_per_s) {
-    if (!c || !radix32_per_s || !radix26_per_s) return MK_ERR_BAD_ARG;
+int mk_measure_field_mul(mk_ctx* c, double* radix32_per_s, double* radix26_per_s, double* radix51_fp64_per_s) {
+    if (!c || !radix32_per_s || !radix26_per_s || !radix51_fp64_per_s) return MK_ERR_BAD_ARG;
     MK_CUDA(c, cudaSetDevice(c->device));
-    MK_CUDA(c, mkb::measure_field_mul_rates((int)c->info.sms, c->stream, radix32_per_s, radix26_per_s));
+    bool exact = false;
+    MK_CUDA(c, mkb::measure_field_mul_rates((int)c->info.sms, c->stream, radix32_per_s, radix26_per_s,
+                                            radix51_fp64_per_s, &exact));
+    if (!exact) return fail(c, MK_ERR_SELF_CHECK, "radix-2^51 (FP64) products differ from radix 2^32");
     return MK_OK;
 }
 

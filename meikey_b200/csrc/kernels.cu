@@ -13,6 +13,9 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
+#include <vector>
+
 #include "ge.cuh"
 #include "hash.cuh"
 #include "kernels.h"
@@ -1059,31 +1062,54 @@ cudaError_t measure_mad_peaks(int sms, cudaStream_t st, double* chain_per_s, dou
 }  // namespace mkb
 
 #include "fe26.cuh"
+#include "fe51.cuh"
 
 namespace mkb {
 
-// Field-multiplication rate of the two limb radices: four independent chains a <- a·b per
+// Field-multiplication rate of three limb radices: four independent chains a <- a·b per
 // thread, no memory traffic.  Radix 2^32 is the search kernel's field (fe32.cuh); radix
-// 2^25.5 (fe26.cuh, ten limbs, 100 mad.wide products) is the alternative the search is not
-// built for.
+// 2^25.5 (fe26.cuh, ten limbs, 100 mad.wide products) and radix 2^51 in FP64 registers
+// (fe51.cuh, five limbs, products split by fused multiply-adds) are the alternatives the
+// search is not built for.  Radices 32 and 51 start from the same words and write the XOR
+// of their chains' canonical words, so their outputs must agree.
 template <int RADIX>
 __global__ void __launch_bounds__(256) k_fe_mul_rate(uint32_t iters, uint32_t seed, uint32_t* out) {
     uint32_t sum = 0;
+    uint32_t wb[8], wa[4][8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) wb[i] = seed * (i + 3) + threadIdx.x;
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+#pragma unroll
+        for (int i = 0; i < 8; i++) wa[q][i] = threadIdx.x * 7 + q * 8 + i;
     if (RADIX == 32) {
-        mk32::fe a[4], b;
+        mk32::fe a[4], b = mk32::fe_from_words(wb);
 #pragma unroll
-        for (int i = 0; i < 8; i++) b.v[i] = seed * (i + 3) + threadIdx.x;
-#pragma unroll
-        for (int q = 0; q < 4; q++)
-#pragma unroll
-            for (int i = 0; i < 8; i++) a[q].v[i] = threadIdx.x * 7 + q * 8 + i;
+        for (int q = 0; q < 4; q++) a[q] = mk32::fe_from_words(wa[q]);
         for (uint32_t it = 0; it < iters; it++)
 #pragma unroll
             for (int q = 0; q < 4; q++) a[q] = mk32::fe_mul(a[q], b);
 #pragma unroll
-        for (int q = 0; q < 4; q++)
+        for (int q = 0; q < 4; q++) {
+            uint32_t w[8];
+            mk32::fe_to_words(a[q], w);
 #pragma unroll
-            for (int i = 0; i < 8; i++) sum ^= a[q].v[i];
+            for (int i = 0; i < 8; i++) sum ^= w[i];
+        }
+    } else if (RADIX == 51) {
+        mk51::fe a[4], b = mk51::fe_from_words(wb);
+#pragma unroll
+        for (int q = 0; q < 4; q++) a[q] = mk51::fe_from_words(wa[q]);
+        for (uint32_t it = 0; it < iters; it++)
+#pragma unroll
+            for (int q = 0; q < 4; q++) a[q] = mk51::fe_mul(a[q], b);
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            uint32_t w[8];
+            mk51::fe_to_words(a[q], w);
+#pragma unroll
+            for (int i = 0; i < 8; i++) sum ^= w[i];
+        }
     } else {
         mk::fe a[4], b;
 #pragma unroll
@@ -1103,35 +1129,55 @@ __global__ void __launch_bounds__(256) k_fe_mul_rate(uint32_t iters, uint32_t se
     out[(uint64_t)blockIdx.x * blockDim.x + threadIdx.x] = sum;
 }
 
-cudaError_t measure_field_mul_rates(int sms, cudaStream_t st, double* radix32_per_s, double* radix26_per_s) {
+cudaError_t measure_field_mul_rates(int sms, cudaStream_t st, double* radix32_per_s, double* radix26_per_s,
+                                    double* radix51_per_s, bool* radix51_exact) {
     const uint32_t blocks = (uint32_t)sms * 8, threads = 256, iters = 1u << 11;
+    const size_t n = (size_t)blocks * threads;
     uint32_t* out = nullptr;
-    cudaError_t e = cudaMalloc(&out, sizeof(uint32_t) * blocks * threads);
+    cudaError_t e = cudaMalloc(&out, sizeof(uint32_t) * n * 2);
     if (e != cudaSuccess) return e;
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    double best[2] = {0, 0};
-    k_fe_mul_rate<32><<<blocks, threads, 0, st>>>(iters / 16, 5u, out);
-    k_fe_mul_rate<26><<<blocks, threads, 0, st>>>(iters / 16, 5u, out);
-    for (int rep = 0; rep < 6 && e == cudaSuccess; rep++) {
-        const int r = rep & 1;
+    double best[3] = {0, 0, 0};
+    auto launch = [&](int r, uint32_t it, uint32_t seed, uint32_t* o) {
+        if (r == 0) k_fe_mul_rate<32><<<blocks, threads, 0, st>>>(it, seed, o);
+        else if (r == 1) k_fe_mul_rate<26><<<blocks, threads, 0, st>>>(it, seed, o);
+        else k_fe_mul_rate<51><<<blocks, threads, 0, st>>>(it, seed, o);
+    };
+    for (int r = 0; r < 3; r++) launch(r, iters / 16, 5u, out);
+    for (int rep = 0; rep < 9 && e == cudaSuccess; rep++) {
+        const int r = rep % 3;
         cudaEventRecord(e0, st);
-        if (r == 0) k_fe_mul_rate<32><<<blocks, threads, 0, st>>>(iters, 9u + rep, out);
-        else k_fe_mul_rate<26><<<blocks, threads, 0, st>>>(iters, 9u + rep, out);
+        launch(r, iters, 9u + rep, out);
         cudaEventRecord(e1, st);
         e = cudaEventSynchronize(e1);
         if (e == cudaSuccess) e = cudaGetLastError();
         float ms = 0;
         if (e == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
-        const double muls = (double)blocks * threads * iters * 4;
+        const double muls = (double)n * iters * 4;
         if (ms > 0 && muls / (ms * 1e-3) > best[r]) best[r] = muls / (ms * 1e-3);
+    }
+    // exactness of radix 2^51: the same chains in radix 2^32 end in the same words
+    bool same = false;
+    if (e == cudaSuccess) {
+        launch(0, 97, 3u, out);
+        launch(2, 97, 3u, out + n);
+        e = cudaStreamSynchronize(st);
+        if (e == cudaSuccess) e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) {
+        std::vector<uint32_t> h(n * 2);
+        e = cudaMemcpy(h.data(), out, sizeof(uint32_t) * n * 2, cudaMemcpyDeviceToHost);
+        same = e == cudaSuccess && std::equal(h.begin(), h.begin() + n, h.begin() + n);
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     cudaFree(out);
     *radix32_per_s = best[0];
     *radix26_per_s = best[1];
+    *radix51_per_s = best[2];
+    *radix51_exact = same;
     return e;
 }
 

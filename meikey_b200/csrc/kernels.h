@@ -46,8 +46,10 @@ constexpr int INCR_STEPS = 16;    // j·B for j = 0 .. keys per thread - 1
 constexpr int INCR_ENTRIES = INCR_WINDOWS * 16 + INCR_STEPS;
 
 cudaError_t launch_keys(const KeyLaunch& L, bool derive, uint32_t kpt, uint32_t block, uint32_t grid, cudaStream_t st);
-// Field multiplications per second in radix 2^32 (the search kernel's) and radix 2^25.5.
-cudaError_t measure_field_mul_rates(int sms, cudaStream_t st, double* radix32_per_s, double* radix26_per_s);
+// Field multiplications per second in radix 2^32 (the search kernel's), radix 2^25.5 and
+// radix 2^51 in FP64; *radix51_exact tells whether radix-2^51 chains matched radix 2^32.
+cudaError_t measure_field_mul_rates(int sms, cudaStream_t st, double* radix32_per_s, double* radix26_per_s,
+                                    double* radix51_per_s, bool* radix51_exact);
 // The kernel of a variant and its dynamic shared memory (for graph nodes); sets the
 // kernel's shared-memory limit like launch_keys does.
 cudaError_t keys_kernel(bool derive, bool incr, uint32_t kpt, uint32_t block, uint32_t hash_warps, uint32_t dfa_smem,

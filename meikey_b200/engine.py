@@ -139,10 +139,12 @@ class Context:
         return a.value, b.value
 
     def measure_field_mul(self):
-        """(radix-2^32, radix-2^25.5) field multiplications per second of the device."""
-        a, b = ctypes.c_double(), ctypes.c_double()
-        _check(self._lib, self._ptr, self._lib.mk_measure_field_mul(self._ptr, ctypes.byref(a), ctypes.byref(b)))
-        return a.value, b.value
+        """(radix-2^32, radix-2^25.5, radix-2^51 FP64) field multiplications per second of the
+        device; raises if the FP64 radix's products differ from radix 2^32's."""
+        a, b, c = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        _check(self._lib, self._ptr,
+               self._lib.mk_measure_field_mul(self._ptr, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
+        return a.value, b.value, c.value
 
     def sync(self):
         _check(self._lib, self._ptr, self._lib.mk_ctx_sync(self._ptr))

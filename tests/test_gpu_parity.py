@@ -431,8 +431,10 @@ def test_autotune_small_space():
 
 
 def test_field_mul_rates(gpu_ctx):
-    r32, r26 = gpu_ctx.measure_field_mul()
-    assert r32 > 1e10 and r26 > 1e10
+    """All three radices run; the FP64 radix-2^51 chains end in the same words as radix 2^32
+    (checked inside the call, which raises on a difference)."""
+    r32, r26, r51 = gpu_ctx.measure_field_mul()
+    assert r32 > 1e10 and r26 > 1e10 and r51 > 1e10
 
 
 def test_incremental_range_must_not_wrap(gpu_ctx):
