@@ -23,6 +23,7 @@ struct mk_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
     cudaStream_t side = nullptr;     // stop requests, written while a launch runs on `stream`
+    cudaMemPool_t pool = nullptr;    // job buffers (stream-ordered, kept across jobs)
     cudaEvent_t ev[16] = {};
     mk_info info{};
     CombGeom geom{};
@@ -66,6 +67,27 @@ struct mk_graph {
 };
 
 namespace {
+
+// Job buffers come from the context's stream-ordered pool.  A released job's memory stays in
+// the pool for the next job, so making and releasing a job neither maps nor unmaps device
+// memory; cudaFree synchronizes the whole device and took tens of milliseconds per job.
+// An allocation is ordered on the context's stream: callers synchronize that stream before
+// another stream or a blocking copy touches the buffer.
+template <class T>
+bool pool_alloc(mk_ctx* c, T** p, size_t bytes) {
+    void* q = nullptr;
+    if (cudaMallocFromPoolAsync(&q, bytes, c->pool, c->stream) != cudaSuccess) {
+        cudaGetLastError();
+        *p = nullptr;
+        return false;
+    }
+    *p = (T*)q;
+    return true;
+}
+
+void pool_free(mk_ctx* c, void* p) {
+    if (p) cudaFreeAsync(p, c->stream);
+}
 
 int fail(mk_ctx* c, int code, const std::string& msg) {
     if (c) c->err = msg;
@@ -221,6 +243,15 @@ int mk_ctx_create(int device, const mk_options* options, mk_ctx** out) {
     MK_CUDA(c, cudaSetDevice(device));
     MK_CUDA(c, cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     MK_CUDA(c, cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
+    {
+        cudaMemPoolProps pp = {};
+        pp.allocType = cudaMemAllocationTypePinned;
+        pp.location.type = cudaMemLocationTypeDevice;
+        pp.location.id = device;
+        MK_CUDA(c, cudaMemPoolCreate(&c->pool, &pp));
+        uint64_t keep = ~0ull;  // freed blocks stay in the pool until the context goes
+        MK_CUDA(c, cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &keep));
+    }
     for (auto& ev : c->ev) MK_CUDA(c, cudaEventCreate(&ev));
     cudaDeviceProp prop;
     MK_CUDA(c, cudaGetDeviceProperties(&prop, device));
@@ -293,6 +324,7 @@ void mk_ctx_destroy(mk_ctx* c) {
         if (ev) cudaEventDestroy(ev);
     if (c->side) cudaStreamDestroy(c->side);
     if (c->stream) cudaStreamDestroy(c->stream);
+    if (c->pool) cudaMemPoolDestroy(c->pool);
     delete c;
 }
 
@@ -510,31 +542,35 @@ static int upload_needles(mk_job* j, mkb::MatchSet& ms, std::vector<mkh25519::Ne
     mk_ctx* c = j->ctx;
     MK_CUDA(c, cudaStreamSynchronize(c->stream));
     ms.gram4 = nullptr;
+    // all copies are ordered on the context's stream after the allocations; the stream is
+    // drained before returning, while the host vectors are still alive
     if (!gram4.empty()) {
-        if (!j->d_gram4 && cudaMalloc(&j->d_gram4, gram4.size() * 4) != cudaSuccess) {
-            j->d_gram4 = nullptr;
+        if (!j->d_gram4 && !pool_alloc(c, &j->d_gram4, gram4.size() * 4))
             return fail(c, MK_ERR_OUT_OF_MEMORY, "prefilter allocation");
-        }
-        MK_CUDA(c, cudaMemcpy(j->d_gram4, gram4.data(), gram4.size() * 4, cudaMemcpyHostToDevice));
+        MK_CUDA(c, cudaMemcpyAsync(j->d_gram4, gram4.data(), gram4.size() * 4, cudaMemcpyHostToDevice, c->stream));
         j->h2d += gram4.size() * 4;
         ms.gram4 = j->d_gram4;
     }
-    for (auto d : j->d_dfa) cudaFree(d);
+    for (auto d : j->d_dfa) pool_free(c, d);
     j->d_dfa.clear();
     for (uint32_t r = 0; r < ms.n_regex; r++) {
         const mkh25519::Needle& h = hosts[ms.regex_id[r]];
         uint8_t* d = nullptr;
-        if (cudaMalloc(&d, h.bytes.size()) != cudaSuccess) return fail(c, MK_ERR_OUT_OF_MEMORY, "DFA allocation");
+        if (!pool_alloc(c, &d, h.bytes.size())) {
+            cudaStreamSynchronize(c->stream);
+            return fail(c, MK_ERR_OUT_OF_MEMORY, "DFA allocation");
+        }
         j->d_dfa.push_back(d);
-        MK_CUDA(c, cudaMemcpy(d, h.bytes.data(), h.bytes.size(), cudaMemcpyHostToDevice));
+        MK_CUDA(c, cudaMemcpyAsync(d, h.bytes.data(), h.bytes.size(), cudaMemcpyHostToDevice, c->stream));
         j->h2d += h.bytes.size();
         ms.dfa[r] = d;
     }
-    if (!j->d_match && cudaMalloc(&j->d_match, sizeof ms) != cudaSuccess) {
-        j->d_match = nullptr;
+    if (!j->d_match && !pool_alloc(c, &j->d_match, sizeof ms)) {
+        cudaStreamSynchronize(c->stream);
         return fail(c, MK_ERR_OUT_OF_MEMORY, "match allocation");
     }
-    MK_CUDA(c, cudaMemcpy(j->d_match, &ms, sizeof ms, cudaMemcpyHostToDevice));
+    MK_CUDA(c, cudaMemcpyAsync(j->d_match, &ms, sizeof ms, cudaMemcpyHostToDevice, c->stream));
+    MK_CUDA(c, cudaStreamSynchronize(c->stream));
     j->h2d += sizeof ms;
     j->needles = std::move(hosts);
     return MK_OK;
@@ -569,11 +605,13 @@ int mk_job_prepare(mk_ctx* c, const uint8_t key[32], int seed_source, const mk_n
         mk_job_destroy(j);
         return fail(c, st, keep);
     }
-    if (cudaMalloc(&j->d_hits, sizeof(mkb::HitRecord) * j->cap) != cudaSuccess) return bail(MK_ERR_OUT_OF_MEMORY, "hit ring");
-    if (cudaMalloc(&j->d_job, sizeof(mkb::JobDevice)) != cudaSuccess) return bail(MK_ERR_OUT_OF_MEMORY, "job state");
-    if (cudaMemset(j->d_job, 0, sizeof(mkb::JobDevice)) != cudaSuccess) return bail(MK_ERR_CUDA, "job state");
-    if (cudaMalloc(&j->d_sink, sizeof(uint32_t) * (size_t)c->grid * c->block) != cudaSuccess)
-        return bail(MK_ERR_OUT_OF_MEMORY, "sink");
+    if (!pool_alloc(c, &j->d_hits, sizeof(mkb::HitRecord) * j->cap)) return bail(MK_ERR_OUT_OF_MEMORY, "hit ring");
+    if (!pool_alloc(c, &j->d_job, sizeof(mkb::JobDevice))) return bail(MK_ERR_OUT_OF_MEMORY, "job state");
+    if (cudaMemsetAsync(j->d_job, 0, sizeof(mkb::JobDevice), c->stream) != cudaSuccess)
+        return bail(MK_ERR_CUDA, "job state");
+    if (!pool_alloc(c, &j->d_sink, sizeof(uint32_t) * (size_t)c->grid * c->block)) return bail(MK_ERR_OUT_OF_MEMORY, "sink");
+    // the side stream (stop requests) and blocking copies may touch the buffers from here on
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) return bail(MK_ERR_CUDA, "job buffers");
     *out = j;
     return MK_OK;
 }
@@ -602,13 +640,17 @@ int mk_job_update(mk_job* j, const mk_needle* needles, uint32_t n_needles) {
 void mk_job_destroy(mk_job* j) {
     if (!j) return;
     if (j->ctx) cudaSetDevice(j->ctx->device);
-    if (j->ctx && j->ctx->stream) cudaStreamSynchronize(j->ctx->stream);
-    for (auto d : j->d_dfa) cudaFree(d);
-    if (j->d_gram4) cudaFree(j->d_gram4);
-    if (j->d_match) cudaFree(j->d_match);
-    if (j->d_hits) cudaFree(j->d_hits);
-    if (j->d_job) cudaFree(j->d_job);
-    if (j->d_sink) cudaFree(j->d_sink);
+    if (j->ctx && j->ctx->stream) {
+        mk_ctx* c = j->ctx;
+        cudaStreamSynchronize(c->stream);
+        cudaStreamSynchronize(c->side);  // a stop request still in flight writes d_job
+        for (auto d : j->d_dfa) pool_free(c, d);
+        pool_free(c, j->d_gram4);
+        pool_free(c, j->d_match);
+        pool_free(c, j->d_hits);
+        pool_free(c, j->d_job);
+        pool_free(c, j->d_sink);
+    }
     delete j;
 }
 
