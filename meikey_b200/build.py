@@ -12,7 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmeikey_b200.so")
 SOURCES = ["kernels.cu", "api.cpp", "host25519.cpp", "regex.cpp", "tune.cpp", "serve.cpp", "keyfile.cpp"]
-HEADERS = ["fe32.cuh", "fe26.cuh", "fe51.cuh", "ge.cuh", "hash.cuh", "kernels.h", "types.h", "host25519.h"]
+HEADERS = ["fe32.cuh", "fe26.cuh", "fe51.cuh", "ge.cuh", "hash.cuh", "kernels.h", "types.h", "host25519.h", "hitsort.h"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -4,16 +4,19 @@
 // the compiled needles and its hit ring.  Every entry point returns a status and
 // records the text of a failure in the context (no exceptions cross the ABI).
 #include <cuda_runtime.h>
+#include <stddef.h>
 #include <stdio.h>
 #include <string.h>
 
 #include <algorithm>
+#include <functional>
 #include <memory>
 #include <new>
 #include <string>
 #include <vector>
 
 #include "../../include/meikey_b200.h"
+#include "hitsort.h"
 #include "host25519.h"
 #include "kernels.h"
 
@@ -24,6 +27,7 @@ struct mk_ctx {
     cudaStream_t stream = nullptr;
     cudaStream_t side = nullptr;     // stop requests, written while a launch runs on `stream`
     cudaMemPool_t pool = nullptr;    // job buffers (stream-ordered, kept across jobs)
+    std::vector<mkhits::HitBuf> spare_hits;  // host hit buffers of released jobs
     cudaEvent_t ev[16] = {};
     mk_info info{};
     CombGeom geom{};
@@ -49,7 +53,8 @@ struct mk_job {
     uint32_t cap = 1u << 16;
     mkb::JobDevice* d_job = nullptr;
     uint32_t* d_sink = nullptr;
-    std::vector<mk_hit> last;
+    mkhits::HitBuf last;     // hits of the last launch (ordered only when `sorted`)
+    bool sorted = true;
     uint32_t last_total = 0;
     uint64_t h2d = 0, d2h = 0;  // bytes copied for this job
 };
@@ -592,6 +597,10 @@ int mk_job_prepare(mk_ctx* c, const uint8_t key[32], int seed_source, const mk_n
     mk_job* j = new (std::nothrow) mk_job;
     if (!j) return fail(c, MK_ERR_OUT_OF_MEMORY, "host allocation");
     j->ctx = c;
+    if (!c->spare_hits.empty()) {
+        j->last = std::move(c->spare_hits.back());
+        c->spare_hits.pop_back();
+    }
     memcpy(j->key, key, 32);
     j->source = seed_source;
     j->stop_on_hit = stop_on_hit;
@@ -650,6 +659,10 @@ void mk_job_destroy(mk_job* j) {
         pool_free(c, j->d_hits);
         pool_free(c, j->d_job);
         pool_free(c, j->d_sink);
+        if (j->last.cap && c->spare_hits.size() < 4) {
+            j->last.clear();
+            c->spare_hits.push_back(std::move(j->last));
+        }
     }
     delete j;
 }
@@ -718,15 +731,20 @@ static int collect(mk_job* j, int* found, uint64_t* index) {
     j->last_total = jd.hit_count;
     uint32_t n = std::min(jd.hit_count, j->cap);
     if (n) {
-        std::vector<mkb::HitRecord> h(n);
-        MK_CUDA(c, cudaMemcpy(h.data(), j->d_hits, sizeof(mkb::HitRecord) * n, cudaMemcpyDeviceToHost));
-        j->d2h += sizeof(mkb::HitRecord) * n;
-        j->last.resize(n);
-        for (uint32_t i = 0; i < n; i++) j->last[i] = mk_hit{h[i].index, h[i].needle, 0};
-        std::sort(j->last.begin(), j->last.end(),
-                  [](const mk_hit& a, const mk_hit& b) { return a.index != b.index ? a.index < b.index : a.needle < b.needle; });
+        static_assert(sizeof(mkb::HitRecord) == sizeof(mk_hit) && offsetof(mkb::HitRecord, needle) == offsetof(mk_hit, needle),
+                      "device hit records are read back as mk_hit");
+        j->last.resize_uninit(n);
+        MK_CUDA(c, cudaMemcpy(j->last.data(), j->d_hits, sizeof(mk_hit) * n, cudaMemcpyDeviceToHost));
+        j->d2h += sizeof(mk_hit) * n;
+        j->sorted = false;
+        uint64_t lowest = ~0ull;
+        mk_hit* h = j->last.data();
+        for (uint32_t i = 0; i < n; i++) {
+            h[i].reserved = 0;
+            lowest = std::min(lowest, h[i].index);
+        }
         if (found) *found = 1;
-        if (index) *index = j->last[0].index;
+        if (index) *index = lowest;
     }
     if (jd.hit_count > j->cap) return fail(c, MK_ERR_HIT_RING_FULL, "hit ring overflow");
     if (jd.status & 1u) return MK_ERR_STOPPED;
@@ -756,8 +774,12 @@ int mk_job_launch(mk_job* j, uint64_t base, uint32_t iters, int* found, uint64_t
 int mk_job_hits(mk_job* j, mk_hit* out, uint32_t cap, uint32_t* written, uint64_t* total) {
     if (!j || !written || !total || (cap && !out)) return MK_ERR_BAD_ARG;
     *total = j->last_total;
-    uint32_t k = std::min<uint32_t>(cap, (uint32_t)j->last.size());
-    for (uint32_t i = 0; i < k; i++) out[i] = j->last[i];
+    uint32_t k = std::min<uint32_t>(cap, (uint32_t)j->last.n);
+    if (k && !j->sorted) {
+        mkhits::sort_hits(j->last.data(), j->last.n);
+        j->sorted = true;
+    }
+    if (k) memcpy(out, j->last.data(), sizeof(mk_hit) * k);
     *written = k;
     return j->last_total > j->cap ? MK_ERR_HIT_RING_FULL : MK_OK;
 }
@@ -796,17 +818,37 @@ int mk_job_first_matches(mk_job* j, mk_outcome* out, uint32_t n) {
         out[k].status = MK_ERR_STOPPED;
         out[k].needle = k;
     }
-    std::vector<char> done(n, 0);
-    for (const mk_hit& h : j->last) {  // sorted by index
-        if (h.needle >= n || done[h.needle]) continue;
-        mk_outcome& o = out[h.needle];
-        int ok = 0;
-        int st = mk_job_confirm(j, h.index, h.needle, o.pk, o.secret, &ok);
-        if (st != MK_OK) return st;
-        if (ok) {
-            o.status = MK_OK;
-            o.index = h.index;
-            done[h.needle] = 1;
+    // per needle, its candidates from the lowest index up until one matches with its real x
+    // sign: the candidates are bucketed by needle and each bucket is a min-heap, so a needle
+    // that confirms at once costs no ordering of the rest
+    const mk_hit* h = j->last.data();
+    const size_t m = j->last.n;
+    std::vector<size_t> start(n + 1, 0);
+    for (size_t i = 0; i < m; i++)
+        if (h[i].needle < n) start[h[i].needle + 1]++;
+    for (uint32_t k = 0; k < n; k++) start[k + 1] += start[k];
+    std::vector<uint64_t>& idx = j->last.scratch;
+    idx.resize(start[n]);
+    {
+        std::vector<size_t> next(start.begin(), start.end() - 1);
+        for (size_t i = 0; i < m; i++)
+            if (h[i].needle < n) idx[next[h[i].needle]++] = h[i].index;
+    }
+    for (uint32_t k = 0; k < n; k++) {
+        auto b = idx.begin() + start[k], e = idx.begin() + start[k + 1];
+        std::make_heap(b, e, std::greater<uint64_t>());
+        while (b != e) {
+            std::pop_heap(b, e, std::greater<uint64_t>());
+            --e;
+            mk_outcome& o = out[k];
+            int ok = 0;
+            int st = mk_job_confirm(j, *e, k, o.pk, o.secret, &ok);
+            if (st != MK_OK) return st;
+            if (ok) {
+                o.status = MK_OK;
+                o.index = *e;
+                break;
+            }
         }
     }
     return MK_OK;

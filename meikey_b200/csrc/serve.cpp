@@ -24,6 +24,7 @@
 #include <vector>
 
 #include "../../include/meikey_b200.h"
+#include "hitsort.h"
 
 namespace {
 
@@ -335,8 +336,7 @@ extern "C" int mk_server_tick(mk_server* s, uint32_t* active, uint32_t* queued) 
         if (int e = fetch_hits(s->job, part)) return e;
         hits.insert(hits.end(), part.begin(), part.end());
     }
-    std::sort(hits.begin(), hits.end(),
-              [](const mk_hit& a, const mk_hit& b) { return a.index != b.index ? a.index < b.index : a.needle < b.needle; });
+    mkhits::sort_hits(hits);
     // per job, in index order: the first candidate that matches with its real x sign
     std::vector<char> closed(s->active.size(), 0);
     uint8_t pk[32], secret[32];

@@ -23,3 +23,15 @@ def test_c_program_against_header(tmp_path):
     out = subprocess.run([str(exe), pk], capture_output=True, text=True)
     assert out.returncode == 0, out.stdout + out.stderr
     assert out.stdout.count("ok ") == 8
+
+
+@pytest.mark.skipif(shutil.which("g++") is None, reason="g++ not installed")
+def test_hit_order_radix_sort(tmp_path):
+    """The library's host-side ordering of candidate hits (radix sort on index, then needle)
+    equals a comparison sort on random, duplicate, constant, wide and nearly sorted sets."""
+    exe = tmp_path / "hitsort_check"
+    subprocess.run(["g++", "-std=c++17", "-O2", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "c", "hitsort_check.cpp"), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert out.stdout.count("ok ") == 11

@@ -510,3 +510,18 @@ def test_prefilter_finds_needles_cut_from_keys(gpu_ctx, oracle):
         assert got == oracle.match_keys(pks, base, nd.text, len(nd.text), nd.fold, nd.mode), k
         if k < len(sources):
             assert sources[k] in got, k
+
+
+def test_large_hit_set_in_index_order(gpu_ctx, oracle):
+    """Tens of thousands of candidates of two needles in one launch come back ordered by
+    (index, needle) (the host's radix path), equal to the oracle's candidate lists."""
+    key = chacha_key(36)
+    kpi = gpu_ctx.keys_per_iter
+    needles = [mk.Needle.contains("ab", case_sensitive=False), mk.Needle.suffix("Q")]
+    with gpu_ctx.job(key, mk.SEED_CHACHA20, needles) as job:
+        job.launch(1000, 1)
+        hits, total = job.hits(cap=1 << 18)
+    want0 = oracle.search(key, 0, 1000, kpi, b"ab", 2, True, 0)
+    want1 = oracle.search(key, 0, 1000, kpi, b"Q", 1, False, 1)
+    assert len(want0) + len(want1) > 4096 and total == len(want0) + len(want1)
+    assert hits == sorted([(i, 0) for i in want0] + [(i, 1) for i in want1])
