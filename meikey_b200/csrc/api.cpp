@@ -483,8 +483,8 @@ static int pack_needles(mk_ctx* c, const mk_needle* needles, uint32_t n_needles,
             uint32_t b = bit + k;
             uint8_t ch = h.bytes[k];
             int v = b64_value(ch);
-            ms.mask[v][b >> 6] |= 1ull << (b & 63);
-            if (h.fold && ch >= 'a' && ch <= 'z') ms.mask[v - 26][b >> 6] |= 1ull << (b & 63);
+            ms.mask[b >> 6][v] |= 1ull << (b & 63);
+            if (h.fold && ch >= 'a' && ch <= 'z') ms.mask[b >> 6][v - 26] |= 1ull << (b & 63);
         }
         ms.first_bit[bit >> 6] |= 1ull << (bit & 63);
         uint32_t last = bit + len - 1;
@@ -536,6 +536,7 @@ static int pack_needles(mk_ctx* c, const mk_needle* needles, uint32_t n_needles,
     }
     ms.sa_words = ms.n_text ? (bit + 63) / 64 : 0;
     if (!prefilter) ms.short_words = ms.sa_words;
+    ms.narrow = ms.n_text && !prefilter && bit <= 32;
     return MK_OK;
 }
 

@@ -219,7 +219,11 @@ __device__ __forceinline__ u32 tail_value(const u32 pk[8], int pos) {
 
 // Tests one key (y only; the character at position 42 is tried with both x signs, as
 // kernel.cu:1804-1875 does) and sets bit `id` of hit_words for every needle that may match.
-__device__ __forceinline__ void match_key(const MatchSet& ms, const u32 pk[8], u64 hit_words[2]) {
+// `lane_masks` (null: none) holds, for jobs whose text needles fit in 32 bits of state, the
+// low half of mask word 0 once per lane (value v of lane l at v * 32 + l): every lane reads
+// its own bank.
+__device__ __forceinline__ void match_key(const MatchSet& ms, const u32* lane_masks, const u32 pk[8],
+                                          u64 hit_words[2]) {
     hit_words[0] = hit_words[1] = 0;
     u32 vals[44];
 #pragma unroll
@@ -241,13 +245,34 @@ __device__ __forceinline__ void match_key(const MatchSet& ms, const u32 pk[8], u
         }
         if (!(any & 1u)) words = ms.short_words;
     }
+    if (lane_masks && words) {
+        const u32* lm = lane_masks + (threadIdx.x & 31u);
+        u32 D = 0, acc = 0;
+        const u32 first = (u32)ms.first_bit[0], last = (u32)ms.last_bit[0];
+#pragma unroll
+        for (int pos = 1; pos < 44; pos++) {
+            u32 mk = lm[vals[pos] * 32u];
+            if (pos == MK_SIGN_POS) mk |= lm[(vals[pos] | 2u) * 32u];
+            D = ((D << 1) | first) & mk;
+            acc |= D & last;
+        }
+        acc |= D & (u32)ms.suffix_bit[0];
+        for (u32 t = 0; acc && t < ms.n_text; t++) {
+            const u32 b = ms.text_last[t];
+            if ((acc >> b) & 1u) {
+                const u32 id = ms.text_id[t];
+                hit_words[id >> 6] |= 1ull << (id & 63);
+            }
+        }
+        words = 0;
+    }
     for (u32 wi = 0; wi < words; wi++) {
         u64 D = 0, acc = 0;
         u64 first = ms.first_bit[wi], last = ms.last_bit[wi];
 #pragma unroll
         for (int pos = 1; pos < 44; pos++) {
-            u64 mk = ms.mask[vals[pos]][wi];
-            if (pos == MK_SIGN_POS) mk |= ms.mask[vals[pos] | 2u][wi];
+            u64 mk = ms.mask[wi][vals[pos]];
+            if (pos == MK_SIGN_POS) mk |= ms.mask[wi][vals[pos] | 2u];
             D = ((D << 1) | first) & mk;
             acc |= D & last;
         }
@@ -387,8 +412,8 @@ __device__ __forceinline__ void combs(const KeyLaunch& L, const CombGeom& g, con
 // Backward pass: `inv` is 1/(product of the batch's denominators); yields each key's
 // canonical y (sign bit 0), tests the needles and reports candidate hits.
 template <int KPT>
-__device__ __forceinline__ void backward(const KeyLaunch& L, const MatchSet& ms, u64 first, const Batch<KPT>& b,
-                                         fe inv, u32& sink) {
+__device__ __forceinline__ void backward(const KeyLaunch& L, const MatchSet& ms, const u32* lane_masks, u64 first,
+                                         const Batch<KPT>& b, fe inv, u32& sink) {
 #pragma unroll 1
     for (int j = KPT - 1; j >= 0; j--) {
         u32 pk[8];
@@ -396,7 +421,7 @@ __device__ __forceinline__ void backward(const KeyLaunch& L, const MatchSet& ms,
         if (j > 0) inv = mk32::fe_mul(inv, b.den[j]);
         sink ^= pk[7];
         u64 hw[2];
-        match_key(ms, pk, hw);
+        match_key(ms, lane_masks, pk, hw);
         const bool any = (hw[0] | hw[1]) != 0;
         // warp ballot: the (rare) warps with a hit compact their records into the ring
         if (__ballot_sync(0xffffffffu, any)) report_hits(hw, first + (u64)j, L.hits, L.hit_cap, L.job);
@@ -524,6 +549,7 @@ __global__ void __launch_bounds__(BLOCK, 512 / BLOCK) k_search(const KeyLaunch L
     EntrySlot* slots = reinterpret_cast<EntrySlot*>(scratch + 2);
     __shared__ CombGeom g;
     __shared__ MatchSet ms;
+    __shared__ u32 lane_masks[64 * 32];  // see match_key
     __shared__ u32 key[8];
     __shared__ mkh::CounterMid mid;
     __shared__ volatile u32 stop_iter;
@@ -565,6 +591,8 @@ __global__ void __launch_bounds__(BLOCK, 512 / BLOCK) k_search(const KeyLaunch L
             }
         }
     }
+    if (ms.narrow)
+        for (u32 i = tid; i < 64u * 32u; i += BLOCK) lane_masks[i] = (u32)ms.mask[0][i >> 5];
     if (tid == 0 && L.seed_src == 1) mid = mkh::counter_mid(key);
     __syncthreads();
     const u32 iters = L.iters;
@@ -619,7 +647,7 @@ __global__ void __launch_bounds__(BLOCK, 512 / BLOCK) k_search(const KeyLaunch L
         const int b = it & 1;
         if (it + 1 < iters && it + 1 < stop_iter) produce(it + 1);
         bar_sync(3 + b, BLOCK);
-        backward<KPT>(L, ms, first_of(it), batch[b], prod[b][tid], sink);
+        backward<KPT>(L, ms, ms.narrow ? lane_masks : nullptr, first_of(it), batch[b], prod[b][tid], sink);
         if (it + 1 >= iters || it + 1 >= stop_iter) break;
     }
     if (L.sink) L.sink[gid] = sink;
@@ -785,7 +813,7 @@ __global__ void __launch_bounds__(BLOCK, 1) k_search_hw(const KeyLaunch L) {
         const int b = it & 1;
         if (it + 1 < iters && it + 1 < stop_iter) produce(it + 1);
         bar_sync(3 + b, B_PIPE);
-        backward<KPT>(L, ms, first_of(it, gid), batch[b], prod[b][tid], sink);
+        backward<KPT>(L, ms, nullptr, first_of(it, gid), batch[b], prod[b][tid], sink);
         if (it + 1 >= iters || it + 1 >= stop_iter) break;
     }
     if (L.sink) L.sink[gid] = sink;

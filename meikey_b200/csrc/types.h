@@ -41,8 +41,11 @@ struct MatchSet {
     uint32_t sa_words;            // words of shift-and state in use
     uint32_t short_words;         // with gram4: the leading words, holding the needles shorter than 4
                                   // characters, that every key scans; the rest only when gram4 fires
-    // shift-and: per value v (0..63) the bits of needle positions accepting v
-    uint64_t mask[64][SA_WORDS];
+    uint32_t narrow;              // 1: the text needles fit in 32 bits of state (word 0, low half)
+    // shift-and: per word and value v (0..63) the bits of needle positions accepting v.  Word
+    // major, so that the 32 lanes' reads of one word at different values spread over the
+    // shared-memory banks (value major, a row of 64 bytes put every lane on bank 0 or 16)
+    uint64_t mask[SA_WORDS][64];
     uint64_t first_bit[SA_WORDS]; // bit 0 of every text needle (set on each step)
     uint64_t last_bit[SA_WORDS];  // last bit of every contains-needle
     uint64_t suffix_bit[SA_WORDS];// last bit of every suffix-needle (tested at the end only)

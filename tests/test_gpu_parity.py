@@ -149,7 +149,8 @@ def test_multi_needle_job_equals_single_jobs(gpu_ctx, golden):
         assert got == case["hits"], n
 
 
-@pytest.mark.parametrize("needle,fold,mode", [("abcd", True, 0), ("Zz", False, 1), ("q+", False, 0)])
+@pytest.mark.parametrize("needle,fold,mode", [("abcd", True, 0), ("Zz", False, 1), ("q+", False, 0), ("x9Q", False, 1),
+                                              ("a/b", True, 0)])
 def test_search_full_launch_matches_oracle(gpu_ctx, oracle, needle, fold, mode):
     """One whole launch (keys_per_iter indices from an odd base) against the oracle."""
     key = chacha_key(7)
@@ -525,3 +526,47 @@ def test_large_hit_set_in_index_order(gpu_ctx, oracle):
     want1 = oracle.search(key, 0, 1000, kpi, b"Q", 1, False, 1)
     assert len(want0) + len(want1) > 4096 and total == len(want0) + len(want1)
     assert hits == sorted([(i, 0) for i in want0] + [(i, 1) for i in want1])
+
+
+@pytest.mark.parametrize("job_no", range(6))
+def test_needles_cut_from_keys_at_every_position(gpu_ctx, oracle, job_no):
+    """Jobs of up to 8 text needles without the 4-gram prefilter: jobs 0-2 (8 needles of 3-8
+    characters) mostly need more than 32 bits of shift-and state (the word-major mask table),
+    jobs 3-5 (4 needles of 2-7) fit in 32 bits (the per-lane table).  Needles cut from known keys at the first and last positions, across the
+    sign-dependent position 42, folded and as suffixes must report their source keys, and
+    every needle's hits must equal the oracle's candidates; a regex needle rides along."""
+    key = chacha_key(45 + job_no)
+    base = 3_000_017 + job_no
+    n = gpu_ctx.keys_per_iter
+    rng = random.Random(45 + job_no)
+    starts = [[0, 1, 2, 3, 4, 5, 6, 7], [33, 34, 35, 36, 37, 38, 39, 40], [10, 21, 30, 38, 39, 40, 40, 39],
+              [0, 1, 39, 40], [37, 38, 2, 41], [20, 40, 39, 3]][job_no]
+    needles, sources = [], []
+    for k, start in enumerate(starts):
+        idx = base + rng.randrange(n)
+        pk = bytearray(oracle.derive(key, 0, idx, 1))
+        pk[31] &= 0x7F  # the y-only key the GPU sees; position 42 is tried with both values
+        hay = oracle.public_b64(bytes(pk))[25:]
+        length = rng.randint(3, 8) if job_no < 3 else rng.randint(2, 7)
+        start = min(start, 43 - length)
+        text = hay[start:start + length]
+        if k % 4 == 1:
+            needles.append(mk.Needle.suffix(hay[43 - length:]))
+        elif k % 4 == 2:
+            needles.append(mk.Needle.contains(text.swapcase(), case_sensitive=False))
+        else:
+            needles.append(mk.Needle.contains(text))
+        sources.append(idx)
+    needles.append(mk.Needle.regex("(ab|cd)[0-9]$"))
+    with gpu_ctx.job(key, mk.SEED_CHACHA20, needles) as job:
+        job.launch(base, 1)
+        hits, total = job.hits(cap=1 << 18)
+    assert total == len(hits)
+    pks = oracle.derive(key, 0, base, n)
+    for k, nd in enumerate(needles):
+        got = [i for i, j in hits if j == k]
+        if nd.mode == 2:
+            assert got == oracle.match_keys(pks, base, nd.text, nd.states, False, 2)
+            continue
+        assert got == oracle.match_keys(pks, base, nd.text, len(nd.text), nd.fold, nd.mode), k
+        assert sources[k] in got, k
