@@ -114,11 +114,18 @@ def workload_key(name: str = "secure") -> bytes:
     return bytes(h)
 
 
+# which part of the multi-pattern workload a run searches: "all" (the workload), or only its
+# "text" patterns or its "regex" patterns (to split the matching cost)
+MULTI_SET = "all"
+
+
 def workload_needle(name: str = "secure") -> str:
     import numpy as np
     w = WORKLOADS[name]
     if name == "multi":
-        return ",".join(t for t, _ in multi_patterns()) + "," + ",".join(MULTI_REGEXES)
+        text = [] if MULTI_SET == "regex" else [t for t, _ in multi_patterns()]
+        rx = [] if MULTI_SET == "text" else list(MULTI_REGEXES)
+        return ",".join(text + rx)
     rng = np.random.default_rng(w["seed"])
     return "".join(ALPHABET[int(i)] for i in rng.integers(0, 64, w["length"]))
 
@@ -127,12 +134,12 @@ def workload_needles(name: str = "secure"):
     import meikey_b200 as mk
     if name == "multi":
         out = []
-        for text, mode in multi_patterns():
+        for text, mode in (multi_patterns() if MULTI_SET != "regex" else []):
             if mode == "suffix":
                 out.append(mk.Needle.suffix(text))
             else:
                 out.append(mk.Needle.contains(text, case_sensitive=mode == "contains"))
-        return out + [mk.Needle.regex(r, max_states=64) for r in MULTI_REGEXES]
+        return out + ([mk.Needle.regex(r, max_states=64) for r in MULTI_REGEXES] if MULTI_SET != "text" else [])
     n = workload_needle(name)
     return [mk.Needle.suffix(n) if WORKLOADS[name]["mode"] == "suffix" else mk.Needle.contains(n)]
 
@@ -636,6 +643,8 @@ def run_ours(args):
         cfg["options_from"] = "mk_autotune sweeps of rows x keys/thread x block (profiles/autotune_sweep.md)"
         cfg["hash_warps"] = args.hash_warps if source != 2 else 0
         cfg["needles"] = len(needles)
+        if args.workload == "multi" and MULTI_SET != "all":
+            cfg["needle_set"] = MULTI_SET + " patterns only"
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -690,7 +699,11 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample length")
     ap.add_argument("--ref-step-seconds", type=float, default=2.0, help="reference arm: seconds per step")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--multi-set", choices=["all", "text", "regex"], default="all",
+                    help="multi-pattern workload: search all its patterns, or only the text or regex ones")
     args = ap.parse_args()
+    global MULTI_SET
+    MULTI_SET = args.multi_set
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "serving":
