@@ -423,7 +423,7 @@ def run_serving(args):
     needles = [needle(t, m) for _, t, m in jobs]
     key = hashlib.sha256(wl["seed"].to_bytes(8, "little")).digest()
     ctx = mk.Context(device=0, table_rows=args.rows, keys_per_thread=args.kpt or 8, block=args.block, self_check=True,
-                     hit_capacity=1 << 22)
+                     hit_capacity=1 << 22, inverter_rotates=args.inverter_rotates)
     budget, iters = wl["budget"], wl["iters_per_tick"]
     # warm-up: a few ticks of a throw-away server
     with mk.Server(ctx, key, max_jobs=4, iters_per_tick=iters, budget=budget, first=1 << 60) as warm:
@@ -540,7 +540,8 @@ def run_ours(args):
     kpt = args.kpt or (16 if source == 2 else 8)
     ctx = mk.Context(device=local, table_rows=args.rows, keys_per_thread=kpt, block=args.block,
                      self_check=True, hit_capacity=(1 << 22) if args.workload == "multi" else 0,
-                     hash_warps=args.hash_warps if source != 2 else 0)
+                     hash_warps=args.hash_warps if source != 2 else 0,
+                     inverter_rotates=args.inverter_rotates)
     kpi = ctx.keys_per_iter
     launches = wl.get("launches", 1)  # > 1: a step is one replay of a CUDA graph of that many launches
     iters = math.ceil((args.step_candidates or wl["step"]) / (kpi * launches))
@@ -642,6 +643,7 @@ def run_ours(args):
         cfg["launches_per_step"] = launches
         cfg["options_from"] = "mk_autotune sweeps of rows x keys/thread x block (profiles/autotune_sweep.md)"
         cfg["hash_warps"] = args.hash_warps if source != 2 else 0
+        cfg["inverter_rotates"] = int(args.inverter_rotates)
         cfg["needles"] = len(needles)
         if args.workload == "multi" and MULTI_SET != "all":
             cfg["needle_set"] = MULTI_SET + " patterns only"
@@ -699,6 +701,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample length")
     ap.add_argument("--ref-step-seconds", type=float, default=2.0, help="reference arm: seconds per step")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--inverter-rotates", action="store_true",
+                    help="every warp derives keys and the inversion rotates over four warps (mk_options.inverter_rotates)")
     ap.add_argument("--multi-set", choices=["all", "text", "regex"], default="all",
                     help="multi-pattern workload: search all its patterns, or only the text or regex ones")
     args = ap.parse_args()

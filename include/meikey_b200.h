@@ -72,13 +72,16 @@ typedef struct mk_options {
     uint32_t table_rows;      /* 10..20; default 12 */
     uint32_t keys_per_thread; /* keys one thread derives before the pooled inversion (default 16) */
     uint32_t block;           /* threads per CTA (default 512): 256 (keys per thread 4, 8, 16) or 512 (8, 16);
-                                 the last warp of a search CTA only inverts */
+                                 see inverter_rotates for who inverts */
     uint32_t blocks_per_sm;   /* resident CTAs per SM the grid is sized for (0 = occupancy maximum) */
     uint32_t self_check;      /* 1: derive keys at creation and compare with the host derivation */
     uint32_t hit_capacity;    /* hit-ring entries per job (0 = 65536) */
     uint32_t hash_warps;      /* 4: search with hashing warps (block 512, keys per thread 8 or 16): 11 comb
                                  warps, 1 inverter, 4 warps computing the SHA-512 scalars, so that hashing
                                  overlaps the comb multiplies; ChaCha20 and counter seeds only.  0: off */
+    uint32_t inverter_rotates;/* 0: a search CTA's last warp only inverts the CTA's products; 1: every warp
+                                 derives keys and the inversion rotates over four warps, one per SM
+                                 sub-partition (pays with long iterations: many needles).  Not with hash_warps */
 } mk_options;
 
 /* One pattern as the reference's GPU needle (Needle, src/service/gpu.rs:618-660):
@@ -110,7 +113,7 @@ typedef struct mk_info {
     uint32_t keys_per_thread;
     uint32_t table_rows;
     uint64_t table_bytes;
-    uint64_t keys_per_iter;   /* grid · (block - 32, or 352 with hash_warps) · keys_per_thread */
+    uint64_t keys_per_iter;   /* grid · (block - 32; block with inverter_rotates; 352 with hash_warps) · keys_per_thread */
     char name[96];
 } mk_info;
 

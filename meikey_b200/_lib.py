@@ -48,6 +48,7 @@ class Options(ctypes.Structure):
         ("self_check", ctypes.c_uint32),
         ("hit_capacity", ctypes.c_uint32),
         ("hash_warps", ctypes.c_uint32),
+        ("inverter_rotates", ctypes.c_uint32),
     ]
 
 

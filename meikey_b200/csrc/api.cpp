@@ -36,6 +36,7 @@ struct mk_ctx {
     uint32_t delta[24] = {};         // keys_per_iter·B (table form)
     uint32_t kpt = 8, block = 256, grid = 0;
     uint32_t hash_warps = 0;  // 4: search kernel with hashing warps (ChaCha20 / counter seeds)
+    uint32_t layout = mkb::LAYOUT_INVERTER_WARP;  // division of work inside a search CTA
     uint32_t hit_capacity = 1u << 16;
     std::string err;
 };
@@ -234,8 +235,9 @@ int mk_ctx_create(int device, const mk_options* options, mk_ctx** out) {
     const bool built = (o.block == 256 && (o.keys_per_thread == 4 || o.keys_per_thread == 8 || o.keys_per_thread == 16)) ||
                        (o.block == 512 && (o.keys_per_thread == 8 || o.keys_per_thread == 16));
     const bool hw_ok = o.hash_warps == 0 || (o.hash_warps == 4 && o.block == 512 && (o.keys_per_thread == 8 || o.keys_per_thread == 16));
-    if (o.table_rows < 10 || o.table_rows > (uint32_t)mkb::MAX_ROWS || !built || !hw_ok || o.blocks_per_sm > 16 ||
-        o.hit_capacity > (1u << 26))
+    const bool rot_ok = o.inverter_rotates <= 1 && !(o.inverter_rotates && o.hash_warps);
+    if (o.table_rows < 10 || o.table_rows > (uint32_t)mkb::MAX_ROWS || !built || !hw_ok || !rot_ok ||
+        o.blocks_per_sm > 16 || o.hit_capacity > (1u << 26))
         return MK_ERR_OUT_OF_RANGE;
     mk_ctx* c = new (std::nothrow) mk_ctx;
     if (!c) return MK_ERR_OUT_OF_MEMORY;
@@ -244,6 +246,7 @@ int mk_ctx_create(int device, const mk_options* options, mk_ctx** out) {
     c->kpt = o.keys_per_thread;
     c->block = o.block;
     c->hash_warps = o.hash_warps;
+    c->layout = o.hash_warps ? mkb::LAYOUT_HASH_WARPS : o.inverter_rotates ? mkb::LAYOUT_ROTATING : mkb::LAYOUT_INVERTER_WARP;
     if (o.hit_capacity) c->hit_capacity = o.hit_capacity;
     MK_CUDA(c, cudaSetDevice(device));
     MK_CUDA(c, cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
@@ -261,7 +264,7 @@ int mk_ctx_create(int device, const mk_options* options, mk_ctx** out) {
     cudaDeviceProp prop;
     MK_CUDA(c, cudaGetDeviceProperties(&prop, device));
     int occ = 0;
-    MK_CUDA(c, mkb::keys_occupancy(false, false, c->kpt, c->block, c->hash_warps, &occ));
+    MK_CUDA(c, mkb::keys_occupancy(false, false, c->kpt, c->block, c->layout, &occ));
     if (occ < 1) return fail(c, MK_ERR_NOT_BUILT, "kernel does not fit on this device");
     uint32_t per_sm = o.blocks_per_sm ? std::min<uint32_t>(o.blocks_per_sm, (uint32_t)occ) : (uint32_t)occ;
     c->grid = (uint32_t)prop.multiProcessorCount * per_sm;
@@ -298,7 +301,7 @@ int mk_ctx_create(int device, const mk_options* options, mk_ctx** out) {
             return fail(c, MK_ERR_OUT_OF_MEMORY, "incremental table allocation failed");
         }
         MK_CUDA(c, cudaMemcpy(c->incr, words.data(), words.size() * 4, cudaMemcpyHostToDevice));
-        mkh25519::niels_of_multiple((uint64_t)c->grid * mkb::search_threads(c->block, c->hash_warps) * c->kpt, c->delta);
+        mkh25519::niels_of_multiple((uint64_t)c->grid * mkb::search_threads(c->block, c->layout) * c->kpt, c->delta);
     }
     // info
     mk_info& in = c->info;
@@ -310,7 +313,7 @@ int mk_ctx_create(int device, const mk_options* options, mk_ctx** out) {
     in.table_rows = c->geom.rows;
     in.table_bytes = bytes;
     // the search kernel's last warp per CTA inverts; the others derive keys
-    in.keys_per_iter = (uint64_t)c->grid * mkb::search_threads(c->block, c->hash_warps) * c->kpt;
+    in.keys_per_iter = (uint64_t)c->grid * mkb::search_threads(c->block, c->layout) * c->kpt;
     snprintf(in.name, sizeof in.name, "%.95s", prop.name);
     if (o.self_check) {
         int st = self_check(c);
@@ -696,7 +699,7 @@ static mkb::KeyLaunch search_params(const mk_job* j, uint64_t base, uint32_t ite
     L.sink = j->d_sink;
     if (j->source == MK_SEED_INCREMENTAL) set_incremental(c, j->key, base, L);
     L.dfa_smem = dfa_smem_bytes(j);
-    L.hash_warps = c->hash_warps;
+    L.layout = c->layout;
     return L;
 }
 
@@ -869,7 +872,7 @@ int mk_ctx_work_per_key(const mk_ctx* c, int seed_source, double* field_muls, do
     // a squaring 28 cross products + 8 diagonal ones (72) + 16
     const double MUL = 144.0, SQ = 88.0;
     const double kpt = c->kpt, rows = c->geom.rows;
-    const double ct = mkb::search_threads(c->block, c->hash_warps), groups = ct / 32.0;
+    const double ct = mkb::search_threads(c->block, c->layout), groups = ct / 32.0;
     // comb: row 0 is free, full additions cost 7 multiplications, the last one 3
     double comb = 7.0 * (rows - 2) + 3.0;
     // Montgomery batch inside a thread: a_j and the running product (2 each for j > 0),
@@ -930,7 +933,7 @@ int mk_job_graph_create(mk_job* j, uint32_t iters, uint32_t launches, mk_graph**
     if (e != cudaSuccess) return bail(e, "cudaGraphAddMemsetNode");
     const void* func = nullptr;
     size_t dyn = 0;
-    e = mkb::keys_kernel(false, j->source == MK_SEED_INCREMENTAL, c->kpt, c->block, c->hash_warps, dfa_smem_bytes(j),
+    e = mkb::keys_kernel(false, j->source == MK_SEED_INCREMENTAL, c->kpt, c->block, c->layout, dfa_smem_bytes(j),
                          &func, &dyn);
     if (e != cudaSuccess) return bail(e, "keys_kernel");
     for (uint32_t i = 0; i < launches; i++) {
@@ -960,7 +963,7 @@ static int graph_enqueue(mk_graph* g, uint64_t base) {
     mk_ctx* c = j->ctx;
     MK_CUDA(c, cudaSetDevice(c->device));
     // the job's needles may have changed since the graph was made: size the DFA staging anew
-    MK_CUDA(c, mkb::keys_kernel(false, j->source == MK_SEED_INCREMENTAL, c->kpt, c->block, c->hash_warps, dfa_smem_bytes(j), &g->func,
+    MK_CUDA(c, mkb::keys_kernel(false, j->source == MK_SEED_INCREMENTAL, c->kpt, c->block, c->layout, dfa_smem_bytes(j), &g->func,
                                 &g->dyn));
     for (size_t i = 0; i < g->nodes.size(); i++) {
         g->params[i] = search_params(j, base + g->span * i, g->iters);

@@ -527,22 +527,31 @@ __device__ __forceinline__ void incr_fracs(const ge& Q, const uint4* steps, Batc
     b.prod = run;
 }
 
-// Search kernel.  The CTA's last warp only inverts; the other BLOCK-32 threads each handle
-// KPT consecutive indices per iteration (index = base + (it·nthreads + gid)·KPT + j, where
-// gid and nthreads count these compute threads).  Iterations are pipelined two deep: a
-// compute thread runs the forward pass of iteration it+1 before the backward pass of it,
-// and the inverter turns the CTA's products of iteration it into their inverses in between.
-// Named barriers: products of buffer b ready (1 + b): compute warps arrive, the inverter
-// waits; inverses of buffer b ready (3 + b): the inverter arrives, compute warps wait.
-// Stop requests (host stop word, or a hit with stop_on_hit) are read by the inverter and
-// take effect two iterations later, at a point every warp agrees on.
+// Search kernel.  The compute threads each handle KPT consecutive indices per iteration
+// (index = base + (it·nthreads + gid)·KPT + j, where gid and nthreads count the compute
+// threads).  Iterations are pipelined two deep: a compute thread runs the forward pass of
+// iteration it+1 before the backward pass of it, and the CTA's products of iteration it are
+// turned into their inverses in between.  Who inverts:
+//   ROT false: the CTA's last warp, which does nothing else (BLOCK-32 compute threads).  The
+//     inversion's long dependent chain runs beside the other warps' work.  That warp's SM
+//     sub-partition (warp w runs on sub-partition w % 4) then holds three compute warps
+//     against four elsewhere;
+//   ROT true: every thread computes keys, and the inversion of iteration it falls to warp
+//     BLOCK/32 - 4 + it % 4, one warp per sub-partition in turn.  The sub-partitions carry
+//     equal shares, but the inverting warp starts its next iteration only after the chain.
+//     That pays when iterations are long (many needles) and costs when they are short.
+// Named barriers, all BLOCK threads: products of buffer b ready (1 + b): the inverting warp
+// waits, the others arrive; inverses of buffer b ready (3 + b): the inverting warp arrives,
+// the others wait.  Stop requests (host stop word, or a hit with stop_on_hit) are read by
+// the inverting warp and take effect two iterations later, at a point every warp agrees on
+// (tests/test_pipeline_protocol.py model-checks the rotating form).
 // INCR: the incremental source.  A compute thread keeps the point Q of its first index in
 // the current iteration; its keys are Q + j·B from the step table, and Q advances by
 // keys_per_iter·B (one mixed addition) per iteration.  No comb table is read.
-template <int KPT, int BLOCK, bool INCR>
+template <int KPT, int BLOCK, bool INCR, bool ROT>
 __global__ void __launch_bounds__(BLOCK, 512 / BLOCK) k_search(const KeyLaunch L) {
-    constexpr int CT = BLOCK - 32;      // compute threads
-    constexpr int CW = CT / 32;         // compute warps = pool length per inverter lane
+    constexpr int CT = ROT ? BLOCK : BLOCK - 32;  // compute threads
+    constexpr int CW = CT / 32;                   // compute warps = pool length per inverting lane
     extern __shared__ uint4 dyn_smem[];
     fe (*prod)[CT] = reinterpret_cast<fe (*)[CT]>(dyn_smem);
     fe (*scratch)[CT] = prod + 2;
@@ -598,8 +607,8 @@ __global__ void __launch_bounds__(BLOCK, 512 / BLOCK) k_search(const KeyLaunch L
     const u32 iters = L.iters;
     if (iters == 0) return;
 
-    if (tid >= (u32)CT) {
-        // ---- inverter warp ----
+    if (!ROT && tid >= (u32)CT) {
+        // ---- dedicated inverter warp ----
         for (u32 it = 0;; it++) {
             const int b = it & 1;
             bar_sync(1 + b, BLOCK);
@@ -621,6 +630,8 @@ __global__ void __launch_bounds__(BLOCK, 512 / BLOCK) k_search(const KeyLaunch L
     }
 
     // ---- compute warps ----
+    const u32 warp = tid >> 5;
+    auto inverts = [&](u32 it) { return ROT && warp == (u32)CW - 4u + (it & 3u); };
     const u64 gid = (u64)blockIdx.x * CT + tid;
     const u64 nthreads = (u64)gridDim.x * CT;
     EntrySlot& slot = slots[INCR ? 0 : tid];
@@ -640,16 +651,33 @@ __global__ void __launch_bounds__(BLOCK, 512 / BLOCK) k_search(const KeyLaunch L
             combs<KPT>(L, g, sc, slot, batch[b]);
         }
         prod[b][tid] = batch[b].prod;
-        bar_arrive(1 + b, BLOCK);
+        if (inverts(it)) {
+            bar_sync(1 + b, BLOCK);
+            if ((tid & 31) == 0) {
+                const volatile JobDevice* jd = L.job;
+                if (jd->stop != 0 || (L.stop_on_hit && jd->hit_count != 0)) {
+                    u32 s = it + 2;
+                    if (s < stop_iter) stop_iter = s;
+                }
+            }
+            __syncwarp();
+            invert_pools(prod[b], scratch[b], CW);
+            __syncwarp();
+            bar_arrive(3 + b, BLOCK);
+        } else {
+            bar_arrive(1 + b, BLOCK);
+        }
     };
     produce(0);
     for (u32 it = 0;; it++) {
         const int b = it & 1;
         if (it + 1 < iters && it + 1 < stop_iter) produce(it + 1);
-        bar_sync(3 + b, BLOCK);
+        if (!inverts(it)) bar_sync(3 + b, BLOCK);
         backward<KPT>(L, ms, ms.narrow ? lane_masks : nullptr, first_of(it), batch[b], prod[b][tid], sink);
         if (it + 1 >= iters || it + 1 >= stop_iter) break;
     }
+    // warp 0 never inverts, so with ROT the last stop decision is visible here
+    if (ROT && tid == 0 && stop_iter < iters) atomicOr(&L.job->status, 1u);
     if (L.sink) L.sink[gid] = sink;
 }
 
@@ -908,13 +936,13 @@ __global__ void __launch_bounds__(BLOCK, 512 / BLOCK) k_derive(const KeyLaunch L
 // dynamic shared memory: products and inversion scratch (two buffers each for the
 // search pipeline) and the per-thread table staging slots
 // (the incremental source reads no comb table and needs no staging slots)
-static size_t dyn_bytes(bool derive, bool incr, uint32_t block, uint32_t hw = 0) {
+static size_t dyn_bytes(bool derive, bool incr, uint32_t block, uint32_t layout) {
     const size_t fe_bytes = 32;
-    if (hw) {  // k_search_hw: 352 comb threads, plus the two-slot scalar ring of 4 keys each
+    if (layout == LAYOUT_HASH_WARPS && !derive && !incr) {  // k_search_hw: 352 comb threads, plus the two-slot scalar ring
         const size_t ct = 352;
         return 4 * ct * fe_bytes + ct * sizeof(EntrySlot) + 2 * 4 * ct * 32;
     }
-    const size_t threads = derive ? block : block - 32;  // the search kernel's last warp only inverts
+    const size_t threads = derive ? block : search_threads(block, layout == LAYOUT_HASH_WARPS ? LAYOUT_INVERTER_WARP : layout);
     return (derive ? 2 : 4) * threads * fe_bytes + (incr ? 0 : threads * sizeof(EntrySlot));
 }
 
@@ -925,11 +953,12 @@ static const void* hw_kernel_of(uint32_t kpt, uint32_t block) {
     return nullptr;
 }
 
-static const void* kernel_of(bool derive, bool incr, uint32_t kpt, uint32_t block) {
-#define MK_FN(K, B)                                                                                        \
-    if (kpt == K && block == B) {                                                                          \
-        if (incr) return derive ? (const void*)k_derive<K, B, true> : (const void*)k_search<K, B, true>;   \
-        return derive ? (const void*)k_derive<K, B, false> : (const void*)k_search<K, B, false>;           \
+static const void* kernel_of(bool derive, bool incr, uint32_t kpt, uint32_t block, bool rot) {
+#define MK_FN(K, B)                                                                                            \
+    if (kpt == K && block == B) {                                                                              \
+        if (derive) return incr ? (const void*)k_derive<K, B, true> : (const void*)k_derive<K, B, false>;      \
+        if (rot) return incr ? (const void*)k_search<K, B, true, true> : (const void*)k_search<K, B, false, true>; \
+        return incr ? (const void*)k_search<K, B, true, false> : (const void*)k_search<K, B, false, false>;    \
     }
     MK_VARIANTS(MK_FN)
 #undef MK_FN
@@ -944,32 +973,32 @@ cudaError_t launch_keys(const KeyLaunch& L, bool derive, uint32_t kpt, uint32_t 
     const bool incr = L.seed_src == SEED_INCREMENTAL;
     if (incr && (kpt > (uint32_t)INCR_STEPS || !L.incr)) return cudaErrorInvalidValue;
     if (L.dfa_smem > DFA_SMEM_MAX || (derive && L.dfa_smem)) return cudaErrorInvalidValue;
-    const bool hw = L.hash_warps && !derive && !incr;
+    const bool hw = L.layout == LAYOUT_HASH_WARPS && !derive && !incr;
     if (hw && L.dfa_smem) return cudaErrorInvalidValue;  // the scalar ring takes that shared memory
-    const void* f = hw ? hw_kernel_of(kpt, block) : kernel_of(derive, incr, kpt, block);
+    const void* f = hw ? hw_kernel_of(kpt, block) : kernel_of(derive, incr, kpt, block, L.layout == LAYOUT_ROTATING);
     if (!f) return cudaErrorInvalidValue;
-    const size_t dyn = dyn_bytes(derive, incr, block, hw ? 4 : 0) + L.dfa_smem;
+    const size_t dyn = dyn_bytes(derive, incr, block, L.layout) + L.dfa_smem;
     cudaError_t e = prepare(f, dyn);
     if (e != cudaSuccess) return e;
     void* args[] = {const_cast<KeyLaunch*>(&L)};
     return cudaLaunchKernel(f, dim3(grid), dim3(block), args, dyn, st);
 }
 
-cudaError_t keys_kernel(bool derive, bool incr, uint32_t kpt, uint32_t block, uint32_t hash_warps, uint32_t dfa_smem,
+cudaError_t keys_kernel(bool derive, bool incr, uint32_t kpt, uint32_t block, uint32_t layout, uint32_t dfa_smem,
                         const void** func, size_t* dyn) {
-    const bool hw = hash_warps && !derive && !incr;
-    const void* f = hw ? hw_kernel_of(kpt, block) : kernel_of(derive, incr, kpt, block);
+    const bool hw = layout == LAYOUT_HASH_WARPS && !derive && !incr;
+    const void* f = hw ? hw_kernel_of(kpt, block) : kernel_of(derive, incr, kpt, block, layout == LAYOUT_ROTATING);
     if (!f || dfa_smem > DFA_SMEM_MAX || (hw && dfa_smem)) return cudaErrorInvalidValue;
     *func = f;
-    *dyn = dyn_bytes(derive, incr, block, hw ? 4 : 0) + dfa_smem;
+    *dyn = dyn_bytes(derive, incr, block, layout) + dfa_smem;
     return prepare(f, *dyn);
 }
 
-cudaError_t keys_occupancy(bool derive, bool incr, uint32_t kpt, uint32_t block, uint32_t hash_warps, int* blocks_per_sm) {
-    const bool hw = hash_warps && !derive && !incr;
-    const void* f = hw ? hw_kernel_of(kpt, block) : kernel_of(derive, incr, kpt, block);
+cudaError_t keys_occupancy(bool derive, bool incr, uint32_t kpt, uint32_t block, uint32_t layout, int* blocks_per_sm) {
+    const bool hw = layout == LAYOUT_HASH_WARPS && !derive && !incr;
+    const void* f = hw ? hw_kernel_of(kpt, block) : kernel_of(derive, incr, kpt, block, layout == LAYOUT_ROTATING);
     if (!f) return cudaErrorInvalidValue;
-    const size_t dyn = dyn_bytes(derive, incr, block, hw ? 4 : 0);
+    const size_t dyn = dyn_bytes(derive, incr, block, layout);
     cudaError_t e = prepare(f, dyn);
     if (e != cudaSuccess) return e;
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, f, (int)block, dyn);

@@ -31,12 +31,19 @@ struct KeyLaunch {
     // bytes of shared memory for the job's DFA tables (each 16-byte aligned; 0: read them
     // from global memory)
     uint32_t dfa_smem;
-    // 4: the search kernel with hashing warps (k_search_hw; ChaCha20 / counter seeds)
-    uint32_t hash_warps;
+    // division of work inside a search CTA (LAYOUT_*)
+    uint32_t layout;
 };
 
-// compute threads of a search CTA: all but the inverter warp, or 11 comb warps with hashing warps
-inline uint32_t search_threads(uint32_t block, uint32_t hash_warps) { return hash_warps ? 352u : block - 32u; }
+// LAYOUT_INVERTER_WARP: the last warp inverts, the others compute keys; LAYOUT_ROTATING: every
+// warp computes keys and the inversion rotates over four warps; LAYOUT_HASH_WARPS: 11 comb
+// warps, 1 inverter, 4 hashing warps (k_search_hw; ChaCha20 / counter seeds)
+constexpr uint32_t LAYOUT_INVERTER_WARP = 0, LAYOUT_ROTATING = 1, LAYOUT_HASH_WARPS = 4;
+
+// compute threads of a search CTA
+inline uint32_t search_threads(uint32_t block, uint32_t layout) {
+    return layout == LAYOUT_HASH_WARPS ? 352u : layout == LAYOUT_ROTATING ? block : block - 32u;
+}
 
 constexpr uint32_t DFA_SMEM_MAX = 48u * 1024u;
 
@@ -52,9 +59,9 @@ cudaError_t measure_field_mul_rates(int sms, cudaStream_t st, double* radix32_pe
                                     double* radix51_per_s, bool* radix51_exact);
 // The kernel of a variant and its dynamic shared memory (for graph nodes); sets the
 // kernel's shared-memory limit like launch_keys does.
-cudaError_t keys_kernel(bool derive, bool incr, uint32_t kpt, uint32_t block, uint32_t hash_warps, uint32_t dfa_smem,
+cudaError_t keys_kernel(bool derive, bool incr, uint32_t kpt, uint32_t block, uint32_t layout, uint32_t dfa_smem,
                         const void** func, size_t* dyn);
-cudaError_t keys_occupancy(bool derive, bool incr, uint32_t kpt, uint32_t block, uint32_t hash_warps, int* blocks_per_sm);
+cudaError_t keys_occupancy(bool derive, bool incr, uint32_t kpt, uint32_t block, uint32_t layout, int* blocks_per_sm);
 // multiply-adds per second of the carry-chain row microbenchmark and of plain mad.lo.u32
 cudaError_t measure_mad_peaks(int sms, cudaStream_t st, double* chain_per_s, double* lo_per_s);
 

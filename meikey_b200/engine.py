@@ -77,10 +77,11 @@ class Context:
     """A device with the comb table built on it (Gpu::new / Kernel::load)."""
 
     def __init__(self, device: int = 0, table_rows: int = 12, keys_per_thread: int = 16, block: int = 512,
-                 blocks_per_sm: int = 0, self_check: bool = False, hit_capacity: int = 0, hash_warps: int = 0):
+                 blocks_per_sm: int = 0, self_check: bool = False, hit_capacity: int = 0, hash_warps: int = 0,
+                 inverter_rotates: bool = False):
         self._lib = L.load()
         opts = L.Options(table_rows, keys_per_thread, block, blocks_per_sm, 1 if self_check else 0, hit_capacity,
-                         hash_warps)
+                         hash_warps, 1 if inverter_rotates else 0)
         ptr = ctypes.c_void_p()
         st = self._lib.mk_ctx_create(device, ctypes.byref(opts), ctypes.byref(ptr))
         self._ptr = ptr
@@ -346,13 +347,15 @@ class Graph:
 BUILT_VARIANTS = [(4, 256), (8, 256), (16, 256), (8, 512), (16, 512)]
 
 
-def tune_space(rows=(11, 12, 13, 14, 16), variants=BUILT_VARIANTS, blocks_per_sm=(0,), hash_warps=(0, 4)):
+def tune_space(rows=(11, 12, 13, 14, 16), variants=BUILT_VARIANTS, blocks_per_sm=(0,), hash_warps=(0, 4),
+               inverter_rotates=(0,)):
     """Candidate options: comb rows (table size against multiplications per key) x keys per
     thread and block (inversion batch = keys per thread x compute warps) x CTAs per SM x the
-    hashing-warp layout (built for block 512, keys per thread 8 and 16)."""
-    return [dict(table_rows=r, keys_per_thread=k, block=b, blocks_per_sm=s, hash_warps=h)
-            for r in rows for (k, b) in variants for s in blocks_per_sm for h in hash_warps
-            if h == 0 or (b == 512 and k in (8, 16))]
+    hashing-warp layout (built for block 512, keys per thread 8 and 16) x who inverts (a
+    dedicated warp, or a duty rotating over four key warps; not with hashing warps)."""
+    return [dict(table_rows=r, keys_per_thread=k, block=b, blocks_per_sm=s, hash_warps=h, inverter_rotates=v)
+            for r in rows for (k, b) in variants for s in blocks_per_sm for h in hash_warps for v in inverter_rotates
+            if (h == 0 or (b == 512 and k in (8, 16))) and not (h and v)]
 
 
 def autotune(device: int = 0, candidates=None, finalists: int = 3, trial_keys: int = 1 << 27):
@@ -362,7 +365,7 @@ def autotune(device: int = 0, candidates=None, finalists: int = 3, trial_keys: i
     arr = (L.TuneEntryC * len(cands))()
     for i, c in enumerate(cands):
         arr[i].options = L.Options(c["table_rows"], c["keys_per_thread"], c["block"], c.get("blocks_per_sm", 0), 1, 0,
-                                   c.get("hash_warps", 0))
+                                   c.get("hash_warps", 0), c.get("inverter_rotates", 0))
     best = ctypes.c_uint32()
     st = lib.mk_autotune(device, arr, len(cands), finalists, trial_keys, ctypes.byref(best))
     if st != L.OK:

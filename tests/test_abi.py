@@ -36,11 +36,11 @@ def test_library_exports_every_declared_symbol():
 
 def test_struct_layouts_match_header():
     from meikey_b200 import _lib
-    assert ctypes.sizeof(_lib.Options) == 28
+    assert ctypes.sizeof(_lib.Options) == 32
     assert ctypes.sizeof(_lib.NeedleC) == 24
     assert ctypes.sizeof(_lib.HitC) == 16
     assert ctypes.sizeof(_lib.InfoC) == 4 * 6 + 16 + 96
-    assert ctypes.sizeof(_lib.TuneEntryC) == 28 + 4 + 4 + 4 + 8  # the double is 8-byte aligned
+    assert ctypes.sizeof(_lib.TuneEntryC) == 32 + 4 + 4 + 8
 
 
 def test_bad_arguments_return_status():
