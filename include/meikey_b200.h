@@ -332,6 +332,14 @@ MK_API int mk_regex_compile(const char* pattern, int case_sensitive, uint32_t ma
 MK_API int mk_autotune(int device, mk_tune_entry* entries, uint32_t n, uint32_t finalists, uint64_t trial_keys,
                        uint32_t* best);
 
+/* mk_autotune timed on the caller's own job instead of the fixed secure-path one: the key,
+ * seed source and needles of mk_job_prepare (the best options depend on the matching work;
+ * inverter_rotates pays with many needles).  A candidate whose job cannot be prepared (e.g.
+ * hash_warps with the incremental source) is dropped with that status. */
+MK_API int mk_autotune_job(int device, mk_tune_entry* entries, uint32_t n, uint32_t finalists, uint64_t trial_keys,
+                           const uint8_t key[32], int seed_source, const mk_needle* needles, uint32_t n_needles,
+                           uint32_t* best);
+
 /* Field multiplications per second on the context's device in radix 2^32 (the search
  * kernel's eight-limb field), radix 2^25.5 (ten limbs, 100 mad.wide products) and radix
  * 2^51 held in FP64 registers (five limbs, products split exactly by fused multiply-adds,

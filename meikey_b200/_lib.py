@@ -152,6 +152,9 @@ SIGNATURES = [
                                         ctypes.POINTER(ctypes.c_uint32), ctypes.c_char_p, ctypes.c_size_t]),
     ("mk_autotune", ctypes.c_int, [ctypes.c_int, ctypes.POINTER(TuneEntryC), ctypes.c_uint32, ctypes.c_uint32,
                                    ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint32)]),
+    ("mk_autotune_job", ctypes.c_int, [ctypes.c_int, ctypes.POINTER(TuneEntryC), ctypes.c_uint32, ctypes.c_uint32,
+                                       ctypes.c_uint64, ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(NeedleC),
+                                       ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32)]),
     ("mk_measure_field_mul", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
                                             ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
     ("mk_job_stop", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),

@@ -3,7 +3,9 @@
 //
 // Stage 1 creates a context for every candidate with the self-check on, so a variant whose
 // keys differ from the host derivation is dropped (MK_ERR_SELF_CHECK), and times one launch
-// of about `trial_keys` secure-path candidates after a warm-up launch.  Stage 2 keeps the
+// of about `trial_keys` candidates after a warm-up launch: of a fixed secure-path job
+// (mk_autotune) or of the caller's own job (mk_autotune_job: seed source, key and needles,
+// since the best options depend on the matching work, e.g. inverter_rotates for many needles).  Stage 2 keeps the
 // `finalists` fastest, holds their contexts together and times them in rounds of
 // alternating order (forward, backward, forward), keeping each one's best rate, so that a
 // drift of the clock over the sweep does not favour whichever ran first.
@@ -27,7 +29,15 @@ struct Live {
     mk_job* job = nullptr;
 };
 
-int open_entry(int device, const mk_options& o, Live& lv) {
+// the job every candidate is timed on
+struct TrialJob {
+    const uint8_t* key;
+    int source;
+    const mk_needle* needles;
+    uint32_t n_needles;
+};
+
+int open_entry(int device, const mk_options& o, const TrialJob& tj, Live& lv) {
     mk_options opt = o;
     opt.self_check = 1;
     int st = mk_ctx_create(device, &opt, &lv.ctx);
@@ -36,8 +46,7 @@ int open_entry(int device, const mk_options& o, Live& lv) {
         lv.ctx = nullptr;
         return st;
     }
-    mk_needle nd{(const uint8_t*)TUNE_NEEDLE, (uint32_t)strlen(TUNE_NEEDLE), 0, MK_MODE_CONTAINS};
-    st = mk_job_prepare(lv.ctx, TUNE_KEY, MK_SEED_CHACHA20, &nd, 1, 0, &lv.job);
+    st = mk_job_prepare(lv.ctx, tj.key, tj.source, tj.needles, tj.n_needles, 0, &lv.job);
     if (st != MK_OK) {
         mk_ctx_destroy(lv.ctx);
         lv.ctx = nullptr;
@@ -67,8 +76,8 @@ int time_launch(Live& lv, uint64_t keys, uint64_t base, double* rate) {
 
 }  // namespace
 
-extern "C" int mk_autotune(int device, mk_tune_entry* entries, uint32_t n, uint32_t finalists, uint64_t trial_keys,
-                           uint32_t* best) {
+static int autotune(int device, mk_tune_entry* entries, uint32_t n, uint32_t finalists, uint64_t trial_keys,
+                    const TrialJob& tj, uint32_t* best) {
     if (!entries || !best || n == 0 || trial_keys == 0) return MK_ERR_BAD_ARG;
     uint64_t base = 1ull << 50;
     // stage 1
@@ -77,7 +86,7 @@ extern "C" int mk_autotune(int device, mk_tune_entry* entries, uint32_t n, uint3
         e.stage = 1;
         e.keys_per_s = 0;
         Live lv;
-        e.status = open_entry(device, e.options, lv);
+        e.status = open_entry(device, e.options, tj, lv);
         if (e.status != MK_OK) continue;
         double warm = 0, rate = 0;
         e.status = time_launch(lv, trial_keys / 4, base, &warm);
@@ -97,7 +106,7 @@ extern "C" int mk_autotune(int device, mk_tune_entry* entries, uint32_t n, uint3
         std::vector<Live> live(order.size());
         int st = MK_OK;
         for (size_t k = 0; k < order.size() && st == MK_OK; k++) {
-            st = open_entry(device, entries[order[k]].options, live[k]);
+            st = open_entry(device, entries[order[k]].options, tj, live[k]);
             entries[order[k]].stage = 2;
             entries[order[k]].keys_per_s = 0;
         }
@@ -117,4 +126,17 @@ extern "C" int mk_autotune(int device, mk_tune_entry* entries, uint32_t n, uint3
     }
     *best = order[0];
     return MK_OK;
+}
+
+extern "C" int mk_autotune(int device, mk_tune_entry* entries, uint32_t n, uint32_t finalists, uint64_t trial_keys,
+                           uint32_t* best) {
+    const mk_needle nd{(const uint8_t*)TUNE_NEEDLE, (uint32_t)strlen(TUNE_NEEDLE), 0, MK_MODE_CONTAINS};
+    return autotune(device, entries, n, finalists, trial_keys, TrialJob{TUNE_KEY, MK_SEED_CHACHA20, &nd, 1}, best);
+}
+
+extern "C" int mk_autotune_job(int device, mk_tune_entry* entries, uint32_t n, uint32_t finalists, uint64_t trial_keys,
+                               const uint8_t key[32], int seed_source, const mk_needle* needles, uint32_t n_needles,
+                               uint32_t* best) {
+    if (!key || (n_needles && !needles)) return MK_ERR_BAD_ARG;
+    return autotune(device, entries, n, finalists, trial_keys, TrialJob{key, seed_source, needles, n_needles}, best);
 }

@@ -358,8 +358,10 @@ def tune_space(rows=(11, 12, 13, 14, 16), variants=BUILT_VARIANTS, blocks_per_sm
             if (h == 0 or (b == 512 and k in (8, 16))) and not (h and v)]
 
 
-def autotune(device: int = 0, candidates=None, finalists: int = 3, trial_keys: int = 1 << 27):
-    """Runs mk_autotune; returns (best options dict, per-candidate results)."""
+def autotune(device: int = 0, candidates=None, finalists: int = 3, trial_keys: int = 1 << 27,
+             job: Optional[Tuple[bytes, int, Sequence[Needle]]] = None):
+    """Runs mk_autotune, or mk_autotune_job when `job` = (key, seed source, needles) gives the
+    workload to time; returns (best options dict, per-candidate results)."""
     lib = L.load()
     cands = candidates or tune_space()
     arr = (L.TuneEntryC * len(cands))()
@@ -367,7 +369,13 @@ def autotune(device: int = 0, candidates=None, finalists: int = 3, trial_keys: i
         arr[i].options = L.Options(c["table_rows"], c["keys_per_thread"], c["block"], c.get("blocks_per_sm", 0), 1, 0,
                                    c.get("hash_warps", 0), c.get("inverter_rotates", 0))
     best = ctypes.c_uint32()
-    st = lib.mk_autotune(device, arr, len(cands), finalists, trial_keys, ctypes.byref(best))
+    if job is None:
+        st = lib.mk_autotune(device, arr, len(cands), finalists, trial_keys, ctypes.byref(best))
+    else:
+        key, source, needles = job
+        narr, keep = _needle_array(list(needles))
+        st = lib.mk_autotune_job(device, arr, len(cands), finalists, trial_keys, bytes(key), source, narr,
+                                 len(needles), ctypes.byref(best))
     if st != L.OK:
         raise GpuError(st, "autotune")
     results = [dict(cands[i], status=arr[i].status, stage=arr[i].stage, keys_per_s=arr[i].keys_per_s)

@@ -570,3 +570,23 @@ def test_needles_cut_from_keys_at_every_position(gpu_ctx, oracle, job_no):
             continue
         assert got == oracle.match_keys(pks, base, nd.text, len(nd.text), nd.fold, nd.mode), k
         assert sources[k] in got, k
+
+
+def test_autotune_on_a_job():
+    """mk_autotune_job times the candidates on the caller's job (here 40 text needles and a
+    regex, where the rotating inversion competes with the dedicated inverter warp); every
+    candidate is self-checked, both reach stage 2, and an incremental job drops the
+    hashing-warp candidate with its preparation status."""
+    from meikey_b200.engine import autotune, tune_space
+    rng = random.Random(9)
+    alphabet = "ABCDEFGHIJKLMNOPQRSTUVWXYZabcdefghijklmnopqrstuvwxyz0123456789+/"
+    needles = [mk.Needle.contains("".join(rng.choice(alphabet) for _ in range(rng.randint(4, 7))))
+               for _ in range(40)] + [mk.Needle.regex("(ab|cd)[0-9]{2}")]
+    space = tune_space(rows=(12,), variants=[(8, 512)], hash_warps=(0,), inverter_rotates=(0, 1))
+    best, results = autotune(0, space, finalists=2, trial_keys=1 << 25, job=(chacha_key(9), mk.SEED_CHACHA20, needles))
+    assert [r["status"] for r in results] == [0, 0] and all(r["stage"] == 2 and r["keys_per_s"] > 1e7 for r in results)
+    assert best["inverter_rotates"] == max(results, key=lambda r: r["keys_per_s"])["inverter_rotates"]
+    space = tune_space(rows=(12,), variants=[(8, 512)], hash_warps=(0, 4))
+    best, results = autotune(0, space, finalists=2, trial_keys=1 << 24,
+                             job=(bytes(range(32, 64)), mk.SEED_INCREMENTAL, [mk.Needle.suffix("Zz")]))
+    assert results[0]["status"] == 0 and results[1]["status"] == mk._lib.ERR_NOT_BUILT and best["hash_warps"] == 0
