@@ -544,7 +544,7 @@ __device__ __forceinline__ void incr_fracs(const ge& Q, const uint4* steps, Batc
 // waits, the others arrive; inverses of buffer b ready (3 + b): the inverting warp arrives,
 // the others wait.  Stop requests (host stop word, or a hit with stop_on_hit) are read by
 // the inverting warp and take effect two iterations later, at a point every warp agrees on
-// (tests/test_pipeline_protocol.py model-checks the rotating form).
+// (tests/test_pipeline_protocol.py model-checks both forms).
 // INCR: the incremental source.  A compute thread keeps the point Q of its first index in
 // the current iteration; its keys are Q + j·B from the step table, and Q advances by
 // keys_per_iter·B (one mixed addition) per iteration.  No comb table is read.

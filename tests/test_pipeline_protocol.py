@@ -1,7 +1,9 @@
-"""CPU model of the search kernel's barrier protocol (csrc/kernels.cu, k_search): every warp
-of a CTA derives keys, and the inversion of iteration it is done by warp W-4+(it mod 4), one
-warp per SM sub-partition in turn.  Named barriers 1+b (products of pipeline buffer b ready)
-and 3+b (their inverses ready), b = it mod 2, count all W warps:
+"""CPU model of the search kernel's barrier protocol (csrc/kernels.cu, k_search), in both of
+its layouts.  Rotating (ROT): every warp of a CTA derives keys, and the inversion of
+iteration it is done by warp W-4+(it mod 4), one warp per SM sub-partition in turn.
+Dedicated (the default): warp W-1 only inverts, every iteration, and the other warps derive
+keys.  Named barriers 1+b (products of pipeline buffer b ready) and 3+b (their inverses
+ready), b = it mod 2, count all W warps:
   - produce(it): a warp writes its product, then arrives on 1+b, except the iteration's
     inverting warp, which syncs on 1+b, inverts, may lower the shared stop iteration to
     it+2, and arrives on 3+b;
@@ -19,6 +21,46 @@ import pytest
 
 def inv_warp(it, warps):
     return warps - 4 + (it & 3)
+
+
+def inverter_program(w, warps, iters, state, stop_at, log):
+    """The dedicated inverter warp: sync on the products, decide on stopping, invert, arrive."""
+    it = 0
+    while True:
+        b = it & 1
+        yield ("sync", 1 + b, it)
+        if it in stop_at:
+            yield ("point",)
+            state["stop"] = min(state["stop"], it + 2)
+        yield ("point",)
+        yield ("arrive", 3 + b, it)
+        log["produced"].append(it)
+        log["done"].append(it)
+        yield ("point",)
+        if it + 1 >= iters or it + 1 >= state["stop"]:
+            return
+        it += 1
+
+
+def compute_program(w, warps, iters, state, stop_at, log):
+    """A key warp of the dedicated layout: arrive on the products, wait for the inverses."""
+    def produce(it):
+        yield ("point",)
+        yield ("arrive", 1 + (it & 1), it)
+        log["produced"].append(it)
+
+    yield from produce(0)
+    it = 0
+    while True:
+        yield ("point",)
+        if it + 1 < iters and it + 1 < state["stop"]:
+            yield from produce(it + 1)
+        yield ("sync", 3 + (it & 1), it)
+        log["done"].append(it)
+        yield ("point",)
+        if it + 1 >= iters or it + 1 >= state["stop"]:
+            return
+        it += 1
 
 
 def warp_program(w, warps, iters, state, stop_at, log):
@@ -52,10 +94,14 @@ def warp_program(w, warps, iters, state, stop_at, log):
         it += 1
 
 
-def run_schedule(warps, iters, stop_at, rng):
+def run_schedule(warps, iters, stop_at, rng, dedicated=False):
     state = {"stop": iters}
     logs = [{"produced": [], "done": []} for _ in range(warps)]
-    progs = [warp_program(w, warps, iters, state, stop_at, logs[w]) for w in range(warps)]
+    if dedicated:
+        progs = [(inverter_program if w == warps - 1 else compute_program)(w, warps, iters, state, stop_at, logs[w])
+                 for w in range(warps)]
+    else:
+        progs = [warp_program(w, warps, iters, state, stop_at, logs[w]) for w in range(warps)]
     blocked = [None] * warps  # barrier a warp waits on
     finished = [False] * warps
     bars = {k: {"n": 0, "tag": None, "waiting": []} for k in (1, 2, 3, 4)}
@@ -98,13 +144,14 @@ def run_schedule(warps, iters, stop_at, rng):
     return length
 
 
+@pytest.mark.parametrize("dedicated", [False, True], ids=["rotating", "dedicated"])
 @pytest.mark.parametrize("warps", [16, 8])
-def test_rotating_inverter_protocol(warps):
-    rng = random.Random(warps)
+def test_inverter_protocol(warps, dedicated):
+    rng = random.Random(warps + 100 * dedicated)
     for trial in range(400):
         iters = rng.choice([1, 2, 3, 4, 5, 7, 9])
         stop_at = {i for i in range(iters) if rng.random() < 0.15}
-        length = run_schedule(warps, iters, stop_at, rng)
+        length = run_schedule(warps, iters, stop_at, rng, dedicated)
         first_stop = min(stop_at) if stop_at else None
         want = iters if first_stop is None else min(iters, first_stop + 2)
         assert length == want, (trial, iters, sorted(stop_at), length)
