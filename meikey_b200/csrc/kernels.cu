@@ -695,7 +695,8 @@ __global__ void __launch_bounds__(BLOCK, 512 / BLOCK) k_search(const KeyLaunch L
 // Whether iteration X is computed is decided, by every role, from the stop word as it stands
 // after the inverter's decision of iteration X-2; the inverter arrives on a decision barrier
 // only when the hashing warps will wait on it, and the hashing warps drain the last two ring
-// releases before they return, so no barrier phase is left open.
+// releases before they return, so no barrier phase is left open (model-checked in
+// tests/test_pipeline_protocol.py).
 template <int KPT, int BLOCK>
 __global__ void __launch_bounds__(BLOCK, 1) k_search_hw(const KeyLaunch L) {
     static_assert(BLOCK == 512 && KPT % 4 == 0 && KPT >= 8, "layout of 11 comb, 1 inverter, 4 hashing warps");
