@@ -713,6 +713,7 @@ __global__ void __launch_bounds__(BLOCK, 1) k_search_hw(const KeyLaunch L) {
     u64 (*ring)[4][CT][4] = reinterpret_cast<u64 (*)[4][CT][4]>(slots + CT);  // [slot][key][thread][word]
     __shared__ CombGeom g;
     __shared__ MatchSet ms;
+    __shared__ u32 lane_masks[64 * 32];  // see match_key
     __shared__ u32 key[8];
     __shared__ mkh::CounterMid mid;
     __shared__ volatile u32 stop_iter;
@@ -729,6 +730,8 @@ __global__ void __launch_bounds__(BLOCK, 1) k_search_hw(const KeyLaunch L) {
         if (tid == 0) stop_iter = L.iters;
     }
     __syncthreads();
+    if (ms.narrow)
+        for (u32 i = tid; i < 64u * 32u; i += BLOCK) lane_masks[i] = (u32)ms.mask[0][i >> 5];
     if (tid == 0 && L.seed_src == 1) mid = mkh::counter_mid(key);
     __syncthreads();
     const u32 iters = L.iters;
@@ -842,7 +845,7 @@ __global__ void __launch_bounds__(BLOCK, 1) k_search_hw(const KeyLaunch L) {
         const int b = it & 1;
         if (it + 1 < iters && it + 1 < stop_iter) produce(it + 1);
         bar_sync(3 + b, B_PIPE);
-        backward<KPT>(L, ms, nullptr, first_of(it, gid), batch[b], prod[b][tid], sink);
+        backward<KPT>(L, ms, ms.narrow ? lane_masks : nullptr, first_of(it, gid), batch[b], prod[b][tid], sink);
         if (it + 1 >= iters || it + 1 >= stop_iter) break;
     }
     if (L.sink) L.sink[gid] = sink;
