@@ -312,7 +312,8 @@ int mk_ctx_create(int device, const mk_options* options, mk_ctx** out) {
     in.keys_per_thread = c->kpt;
     in.table_rows = c->geom.rows;
     in.table_bytes = bytes;
-    // the search kernel's last warp per CTA inverts; the others derive keys
+    // the threads of a search CTA that derive keys (all but a dedicated inverter warp, unless the
+    // inversion rotates; 352 comb threads with hashing warps)
     in.keys_per_iter = (uint64_t)c->grid * mkb::search_threads(c->block, c->layout) * c->kpt;
     snprintf(in.name, sizeof in.name, "%.95s", prop.name);
     if (o.self_check) {

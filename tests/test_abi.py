@@ -78,3 +78,17 @@ def test_missing_library_fails_loudly(tmp_path, monkeypatch):
     monkeypatch.setattr(_lib, "LIB_PATH", str(tmp_path / "missing.so"))
     with pytest.raises(OSError):
         _lib.load()
+
+
+def test_tune_space_candidates_are_context_options():
+    """Every candidate of the tuner's space is a valid keyword set of Context (so that
+    Context(**best) works), hashing warps appear only with block 512 and 8 or 16 keys per
+    thread, and never together with the rotating inversion."""
+    import inspect
+    from meikey_b200.engine import Context, tune_space
+    params = set(inspect.signature(Context.__init__).parameters)
+    space = tune_space(rows=(11, 12), hash_warps=(0, 4), inverter_rotates=(0, 1))
+    assert space and all(set(c) <= params for c in space)
+    assert all(c["block"] == 512 and c["keys_per_thread"] in (8, 16) for c in space if c["hash_warps"])
+    assert not any(c["hash_warps"] and c["inverter_rotates"] for c in space)
+    assert {(c["hash_warps"], c["inverter_rotates"]) for c in space} == {(0, 0), (0, 1), (4, 0)}
