@@ -40,7 +40,7 @@ WORKLOADS = {
     "secure": {"total": 1 << 34, "step": 1 << 30, "source": 0, "seed": 7, "length": 7, "mode": "contains"},
     "incremental": {"total": 1 << 32, "step": 1 << 28, "source": 2, "seed": 11, "length": 6, "mode": "suffix"},
     "multi": {"total": 1 << 34, "step": 1 << 30, "source": 0, "seed": 23, "length": 0, "mode": "mixed",
-              "launches": 4},
+              "launches": 4, "inverter_rotates": True},
     "serving": {"total": 0, "step": 0, "source": 0, "seed": 31, "length": 0, "mode": "mixed", "jobs": 1000,
                 "rate": 50.0, "budget": 1 << 26, "iters_per_tick": 8},
 }
@@ -701,13 +701,17 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample length")
     ap.add_argument("--ref-step-seconds", type=float, default=2.0, help="reference arm: seconds per step")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--inverter-rotates", action="store_true",
-                    help="every warp derives keys and the inversion rotates over four warps (mk_options.inverter_rotates)")
+    ap.add_argument("--inverter-rotates", action=argparse.BooleanOptionalAction, default=None,
+                    help="every warp derives keys and the inversion rotates over four warps "
+                         "(mk_options.inverter_rotates; default: on for the multi-pattern workload, "
+                         "the layout mk_autotune_job picks for it, off otherwise)")
     ap.add_argument("--multi-set", choices=["all", "text", "regex"], default="all",
                     help="multi-pattern workload: search all its patterns, or only the text or regex ones")
     args = ap.parse_args()
     global MULTI_SET
     MULTI_SET = args.multi_set
+    if args.inverter_rotates is None:
+        args.inverter_rotates = bool(WORKLOADS[args.workload].get("inverter_rotates", False))
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "serving":
