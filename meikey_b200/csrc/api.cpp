@@ -9,7 +9,9 @@
 #include <string.h>
 
 #include <algorithm>
+#include <atomic>
 #include <functional>
+#include <thread>
 #include <memory>
 #include <new>
 #include <string>
@@ -789,19 +791,32 @@ int mk_job_hits(mk_job* j, mk_hit* out, uint32_t cap, uint32_t* written, uint64_
     return j->last_total > j->cap ? MK_ERR_HIT_RING_FULL : MK_OK;
 }
 
-int mk_job_confirm(mk_job* j, uint64_t index, uint32_t needle, uint8_t pk[32], uint8_t secret[32], int* matched) {
-    if (!j || !pk || !secret || !matched) return MK_ERR_BAD_ARG;
-    if (needle >= j->needles.size()) return fail(j->ctx, MK_ERR_BAD_ARG, "needle index out of range");
+// Re-derives a candidate on the host and tests its needle with the real x sign.  Touches no
+// shared state (host threads confirm different needles at once); 1 / 2 for a bad needle or
+// start scalar.
+static int confirm_key(const mk_job* j, uint64_t index, uint32_t needle, uint8_t pk[32], uint8_t secret[32],
+                       int* matched) {
+    if (needle >= j->needles.size()) return 1;
     *matched = 0;
     if (j->source == MK_SEED_INCREMENTAL) {
-        if (!mkh25519::incremental_scalar(j->key, index, secret))
-            return fail(j->ctx, MK_ERR_BAD_ARG, "incremental start scalar must be below 2^255");
+        if (!mkh25519::incremental_scalar(j->key, index, secret)) return 2;
         mkh25519::scalar_public_key(secret, pk);
     } else {
         mkh25519::seed_of(j->key, j->source, index, secret);
         mkh25519::public_key(secret, pk);
     }
     *matched = mkh25519::matches(j->needles[needle], pk) ? 1 : 0;
+    return 0;
+}
+
+static int confirm_fail(mk_job* j, int e) {
+    return fail(j->ctx, MK_ERR_BAD_ARG,
+                e == 1 ? "needle index out of range" : "incremental start scalar must be below 2^255");
+}
+
+int mk_job_confirm(mk_job* j, uint64_t index, uint32_t needle, uint8_t pk[32], uint8_t secret[32], int* matched) {
+    if (!j || !pk || !secret || !matched) return MK_ERR_BAD_ARG;
+    if (int e = confirm_key(j, index, needle, pk, secret, matched)) return confirm_fail(j, e);
     return MK_OK;
 }
 
@@ -839,23 +854,37 @@ int mk_job_first_matches(mk_job* j, mk_outcome* out, uint32_t n) {
         for (size_t i = 0; i < m; i++)
             if (h[i].needle < n) idx[next[h[i].needle]++] = h[i].index;
     }
-    for (uint32_t k = 0; k < n; k++) {
-        auto b = idx.begin() + start[k], e = idx.begin() + start[k + 1];
-        std::make_heap(b, e, std::greater<uint64_t>());
-        while (b != e) {
-            std::pop_heap(b, e, std::greater<uint64_t>());
-            --e;
-            mk_outcome& o = out[k];
-            int ok = 0;
-            int st = mk_job_confirm(j, *e, k, o.pk, o.secret, &ok);
-            if (st != MK_OK) return st;
-            if (ok) {
-                o.status = MK_OK;
-                o.index = *e;
-                break;
+    // needles are independent: host threads take them in turn (a confirmation is a host
+    // Ed25519 derivation, tens of microseconds)
+    std::vector<int> errs(n, 0);
+    std::atomic<uint32_t> next{0};
+    auto work = [&]() {
+        for (uint32_t k; (k = next.fetch_add(1)) < n;) {
+            auto b = idx.begin() + start[k], e = idx.begin() + start[k + 1];
+            std::make_heap(b, e, std::greater<uint64_t>());
+            while (b != e) {
+                std::pop_heap(b, e, std::greater<uint64_t>());
+                --e;
+                mk_outcome& o = out[k];
+                int ok = 0;
+                if ((errs[k] = confirm_key(j, *e, k, o.pk, o.secret, &ok)) != 0) break;
+                if (ok) {
+                    o.status = MK_OK;
+                    o.index = *e;
+                    break;
+                }
             }
         }
-    }
+    };
+    uint32_t busy = 0;
+    for (uint32_t k = 0; k < n; k++) busy += start[k + 1] > start[k];
+    const uint32_t threads = std::min<uint32_t>(std::min<uint32_t>(busy, 16u), std::max(1u, std::thread::hardware_concurrency()));
+    std::vector<std::thread> pool;
+    for (uint32_t t = 1; t < threads; t++) pool.emplace_back(work);
+    work();
+    for (auto& t : pool) t.join();
+    for (uint32_t k = 0; k < n; k++)
+        if (errs[k]) return confirm_fail(j, errs[k]);
     return MK_OK;
 }
 

@@ -160,3 +160,31 @@ def test_search_reruns_overflowing_launches(gpu_ctx, oracle):
         narrow = job.search(first=7, iters=1)
     assert wide["found"] and (wide["index"], wide["pk"]) == (narrow["index"], narrow["pk"])
     assert _first_full_match(oracle, key, 0, 7, wide["index"], nd) == wide["index"]
+
+
+def test_first_matches_are_lowest_confirmed_per_needle(gpu_ctx, oracle):
+    """mk_job_first_matches (confirmed on several host threads): for every needle, the lowest
+    candidate of the launch whose key matches with its real x sign, with the oracle's key and
+    seed; needles without a confirmed candidate report STOPPED."""
+    key = chacha_key(37)
+    rng = random.Random(37)
+    needles = [mk.Needle.contains("".join(rng.choice(ALPHABET) for _ in range(3))) for _ in range(24)]
+    needles += [mk.Needle.suffix("Zq9xYw7"), mk.Needle.contains("ab", case_sensitive=False)]
+    with gpu_ctx.job(key, mk.SEED_CHACHA20, needles) as job:
+        job.launch(4242, 1)
+        hits, total = job.hits(cap=1 << 18)
+        outs = job.first_matches()
+    assert total == len(hits) and len(outs) == len(needles)
+    for k, nd in enumerate(needles):
+        cands = [i for i, j in hits if j == k]
+        want = None
+        for i in cands:
+            if oracle.match(oracle.derive(key, 0, i, 1), nd.text, len(nd.text), nd.fold, nd.mode, False):
+                want = i
+                break
+        if want is None:
+            assert outs[k] is None, k
+        else:
+            assert outs[k]["index"] == want, k
+            assert outs[k]["pk"] == oracle.derive(key, 0, want, 1)
+            assert outs[k]["secret"] == oracle.seed(key, 0, want)
