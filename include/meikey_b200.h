@@ -232,7 +232,8 @@ MK_API int mk_job_stop(mk_job* job, int on);
 
 /* For each needle k < n: the lowest candidate of the last launch (or graph replay) that the
  * host confirms (mk_job_confirm, in index order), in out[k] (status MK_OK with index, key and
- * secret; MK_ERR_STOPPED when none of its candidates matches with the real x sign). */
+ * secret; MK_ERR_STOPPED when none of its candidates matches with the real x sign).  Needles
+ * are confirmed on up to 16 host threads of the call's own; it returns when all are done. */
 MK_API int mk_job_first_matches(mk_job* job, mk_outcome* out, uint32_t n);
 
 /* Validates needles as mk_job_prepare would (host only, no device). */
