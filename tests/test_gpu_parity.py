@@ -590,3 +590,16 @@ def test_autotune_on_a_job():
     best, results = autotune(0, space, finalists=2, trial_keys=1 << 24,
                              job=(bytes(range(32, 64)), mk.SEED_INCREMENTAL, [mk.Needle.suffix("Zz")]))
     assert results[0]["status"] == 0 and results[1]["status"] == mk._lib.ERR_NOT_BUILT and best["hash_warps"] == 0
+
+
+def test_empty_needle_set(gpu_ctx, oracle):
+    """A job without needles runs its launches and graph replays and reports nothing; keys
+    derived beside it are unaffected."""
+    key = chacha_key(38)
+    with gpu_ctx.job(key, mk.SEED_CHACHA20, []) as job:
+        assert job.launch(99, 2) is None
+        assert job.hits(cap=16) == ([], 0)
+        with job.graph(1, 2) as g:
+            assert g.launch(7) is None
+        assert job.hits(cap=16) == ([], 0)
+    assert gpu_ctx.derive(key, mk.SEED_CHACHA20, 99, 3) == oracle.derive(key, 0, 99, 3)
