@@ -603,3 +603,18 @@ def test_empty_needle_set(gpu_ctx, oracle):
             assert g.launch(7) is None
         assert job.hits(cap=16) == ([], 0)
     assert gpu_ctx.derive(key, mk.SEED_CHACHA20, 99, 3) == oracle.derive(key, 0, 99, 3)
+
+
+@pytest.mark.parametrize("source", [mk.SEED_CHACHA20, mk.SEED_COUNTER])
+def test_search_ends_at_the_top_of_the_index_space(gpu_ctx, oracle, source):
+    """A launch covering the last keys_per_iter indices below 2^64 (ChaCha20 blocks near 2^63,
+    the counter seed's tail wrapping) finds the oracle's candidates."""
+    key = chacha_key(39 + source)
+    kpi = gpu_ctx.keys_per_iter
+    base = 2**64 - kpi
+    nd = mk.Needle.contains("Ab")
+    with gpu_ctx.job(key, source, [nd]) as job:
+        job.launch(base, 1)
+        hits, total = job.hits(cap=1 << 18)
+    want = oracle.search(key, source, base, kpi, b"Ab", 2, False, 0)
+    assert [i for i, _ in hits] == want and total == len(want)
