@@ -1,27 +1,43 @@
 // Regex -> DFA over the 64 base64 values, in the GPU table layout (the host side of regex
-// needles: src/model/pattern/dfa.rs:52-108 Dfa::new, 189-200 gpu_table).
+// needles: src/model/pattern/dfa.rs:52-108 Dfa::new, 189-200 gpu_table, and the checks of
+// Pattern::regex, src/model/pattern.rs:135-165).
 //
 // Table: `states` rows of 65 little-endian u16.  Row s, column v (0..63) is the next state
 // after the base64 character of value v; column 64 is 1 when the state accepts at the end
 // of the input.  State 0 is the absorbing accept state, state 1 the start.  Matching is an
-// unanchored search over the 43 characters after the fixed key prefix: `^` anchors at the
-// first of them and `$` at the last.
+// unanchored search over the 43 characters after the fixed key prefix, which form the whole
+// haystack: `^` and `\A` anchor at the first of them, `$` and `\z` at the last, and a word
+// boundary at either end sees no word character beyond it.
 //
-// Syntax (a subset of the regex crate's, ASCII patterns): literals, `.`, classes `[...]`
-// with ranges and negation, `\d`, `\w`, escaped metacharacters, groups `(...)` and `(?:...)`,
-// alternation `|`, `*`, `+`, `?`, `{m}`, `{m,}`, `{m,n}`, anchors `^` `$`, and
-// case-insensitive matching (letters match both cases).
+// Dialect: the reference parses with regex-syntax in ASCII mode (unicode(false), utf8(false),
+// case_insensitive(!case_sensitive)), so this compiler follows that grammar:
+//   literals; `.`; classes `[...]` with ranges, negation, nested classes, POSIX classes
+//   `[[:alpha:]]` (and `[[:^alpha:]]`) and the set operations `&&`, `--`, `~~`;
+//   Perl classes \d \D \w \W \s \S (ASCII: \w is [0-9A-Za-z_]);
+//   assertions ^ $ \A \z \b \B \< \> \b{start} \b{end} \b{start-half} \b{end-half};
+//   escapes of ASCII punctuation, \a \f \t \n \r \v, \x7F \x{...} \u.... \u{...} \U........;
+//   groups (...), (?:...), (?P<name>...), (?<name>...), flag groups (?flags) and
+//   (?flags:...) with the flags i m s U u x R (and `-` to clear); alternation;
+//   repetition * + ? {m} {m,} {m,n}, each optionally lazy (a trailing ?).
+// A character outside the base64 alphabet matches nothing.  Everything else the reference's
+// grammar rejects is rejected here too; what it accepts but this compiler does not implement
+// (Unicode classes \p / \P, a Unicode word boundary under the `u` flag) is rejected with an
+// error, never compiled into something else.
 //
-// Construction: a Thompson NFA (one symbol edge or epsilon edges per state, anchors as
+// Construction: a Thompson NFA (one symbol edge or epsilon edges per state; assertions are
 // conditional epsilon edges), then the subset construction with the start state re-added
 // after every character (unanchored search), numbering DFA states in breadth-first order of
-// discovery over the values 0..63.
+// discovery over the values 0..63.  An assertion about the next character (a word boundary,
+// or the end of the haystack) is decided when that character is read: a DFA state also
+// records whether the previous character was a word character, and a match that ends on such
+// an assertion is reported one character later, or by the end-of-input flag.
 #include <stdio.h>
 #include <string.h>
 
+#include <algorithm>
 #include <map>
-#include <set>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "../../include/meikey_b200.h"
@@ -32,7 +48,6 @@ const char ALPHABET[] = "ABCDEFGHIJKLMNOPQRSTUVWXYZabcdefghijklmnopqrstuvwxyz012
 
 typedef unsigned long long u64;
 
-// a set of base64 values as a 64-bit mask
 int value_of(int c) {
     const char* p = (c > 0 && c < 128) ? strchr(ALPHABET, c) : nullptr;
     return p ? (int)(p - ALPHABET) : -1;
@@ -40,57 +55,113 @@ int value_of(int c) {
 
 bool is_alpha(int c) { return (c >= 'A' && c <= 'Z') || (c >= 'a' && c <= 'z'); }
 bool is_digit(int c) { return c >= '0' && c <= '9'; }
+bool is_alnum(int c) { return is_alpha(c) || is_digit(c); }
 
-u64 char_set(int c, bool fold) {
+// base64 values that are ASCII word characters ([0-9A-Za-z_]; '+' and '/' are not)
+const u64 WORD_VALUES = (1ull << 62) - 1;
+
+bool value_is_word(int v) { return v < 62; }
+
+// the base64 values among the ASCII characters lo..hi (one case each)
+u64 range_set(int lo, int hi) {
     u64 m = 0;
-    auto add = [&](int x) {
-        int v = value_of(x);
+    for (int c = std::max(lo, 1); c <= std::min(hi, 127); c++) {
+        int v = value_of(c);
         if (v >= 0) m |= 1ull << v;
-    };
-    if (fold && is_alpha(c)) {
-        add(c | 0x20);
-        add(c & ~0x20);
-    } else {
-        add(c);
     }
     return m;
 }
 
+// simple case folding of a set of values: every letter brings its other case
+u64 fold_set(u64 m) {
+    u64 r = m;
+    for (int v = 0; v < 52; v++)
+        if ((m >> v) & 1) r |= 1ull << (v < 26 ? v + 26 : v - 26);
+    return r;
+}
+
 struct Node {
-    enum Kind { SET, BOL, EOL, CAT, ALT, REP } kind;
+    enum Kind { SET, LOOK, CAT, ALT, REP } kind = CAT;
     u64 set = 0;
+    int look = 0;  // LOOK: one of the Look kinds
     std::vector<Node> kids;
     int lo = 0, hi = 0;  // REP: hi < 0 means unbounded
 };
+
+// zero-width assertions (conditional epsilon edges of the NFA)
+enum Look {
+    L_START = 1,       // ^ \A: at the first character of the haystack
+    L_END,             // $ \z: after its last character
+    L_WORD,            // \b: word character on exactly one side
+    L_NOT_WORD,        // \B: word characters on both sides or on neither
+    L_WORD_START,      // \< \b{start}: no word character before, one after
+    L_WORD_END,        // \> \b{end}: a word character before, none after
+    L_WORD_START_HALF, // \b{start-half}: no word character before
+    L_WORD_END_HALF,   // \b{end-half}: no word character after
+};
+
+bool is_word_look(int k) { return k >= L_WORD; }
 
 struct Error {
     std::string msg;
 };
 
+struct Flags {
+    bool i = false, m = false, s = false, U = false, u = false, x = false, R = false;
+};
+
 struct Parser {
     const std::string& s;
     size_t i = 0;
-    bool fold;
-    Parser(const std::string& str, bool f) : s(str), fold(f) {}
+    Flags f;
+    int depth = 0;
+    Parser(const std::string& str, bool fold) : s(str) { f.i = fold; }
 
+    [[noreturn]] void error(const std::string& m) { throw Error{m}; }
+    bool eof() const { return i >= s.size(); }
     int peek() const { return i < s.size() ? (unsigned char)s[i] : -1; }
+    int peek_at(size_t k) const { return i + k < s.size() ? (unsigned char)s[i + k] : -1; }
     int take() {
-        if (i >= s.size()) throw Error{"unexpected end of pattern"};
+        if (i >= s.size()) error("unexpected end of pattern");
         return (unsigned char)s[i++];
+    }
+    // verbose mode (x): whitespace and #-comments between tokens are ignored
+    void skip_space() {
+        if (!f.x) return;
+        for (;;) {
+            int c = peek();
+            if (c == ' ' || c == '\t' || c == '\n' || c == '\r' || c == '\f' || c == '\v') {
+                i++;
+            } else if (c == '#') {
+                while (!eof() && s[i] != '\n') i++;
+            } else {
+                return;
+            }
+        }
     }
 
     Node parse() {
         Node n = alt();
-        if (peek() != -1) throw Error{std::string("unexpected '") + (char)peek() + "'"};
+        if (!eof()) {
+            if (peek() == ')') error("unopened group");
+            error(std::string("unexpected '") + (char)peek() + "'");
+        }
         return n;
     }
+    void enter() {
+        if (++depth > 250) error("nest limit exceeded");
+    }
     Node alt() {
+        enter();
         std::vector<Node> parts;
+        Flags saved = f;  // flags set inside a group end with it
         parts.push_back(concat());
         while (peek() == '|') {
             take();
             parts.push_back(concat());
         }
+        f = saved;
+        depth--;
         if (parts.size() == 1) return parts[0];
         Node n;
         n.kind = Node::ALT;
@@ -100,8 +171,47 @@ struct Parser {
     Node concat() {
         Node n;
         n.kind = Node::CAT;
-        while (peek() != -1 && peek() != '|' && peek() != ')') n.kids.push_back(repeat());
+        for (;;) {
+            skip_space();
+            if (eof() || peek() == '|' || peek() == ')') break;
+            if (peek() == '(' && peek_at(1) == '?' && flag_group_ahead()) {
+                // (?flags): applies to the rest of the enclosing group
+                i += 2;
+                parse_flags(')');
+                continue;
+            }
+            n.kids.push_back(repeat());
+        }
         return n;
+    }
+    // "(?" starts a flag group without a body: flags then ')'
+    bool flag_group_ahead() const {
+        size_t j = i + 2;
+        while (j < s.size() && strchr("imsUuxR-", s[j])) j++;
+        return j < s.size() && s[j] == ')';
+    }
+    // flags up to `end` (':' or ')'), which is consumed
+    void parse_flags(int end) {
+        bool neg = false, any = false, after_neg = false;
+        for (;;) {
+            int c = take();
+            if (c == end) break;
+            if (c == ':' || c == ')') error("bad flag group");
+            if (c == '-') {
+                if (neg) error("repeated negation in a flag group");
+                neg = true;
+                after_neg = false;
+                continue;
+            }
+            bool* fl = c == 'i' ? &f.i : c == 'm' ? &f.m : c == 's' ? &f.s : c == 'U' ? &f.U
+                     : c == 'u' ? &f.u : c == 'x' ? &f.x : c == 'R' ? &f.R : nullptr;
+            if (!fl) error(std::string("unrecognized flag '") + (char)c + "'");
+            *fl = !neg;
+            any = true;
+            after_neg = neg;
+        }
+        if (!any && end == ')') error("empty flag group");
+        if (neg && !after_neg) error("dangling flag negation");
     }
     static Node rep(Node sub, int lo, int hi) {
         Node n;
@@ -111,118 +221,318 @@ struct Parser {
         n.kids.push_back(std::move(sub));
         return n;
     }
+    int decimal() {
+        size_t st = i;
+        long v = 0;
+        while (is_digit(peek())) {
+            v = v * 10 + (take() - '0');
+            if (v > 100000) error("repetition quantifier is too large");
+        }
+        if (i == st) error("bad repetition: a count is missing");
+        return (int)v;
+    }
     Node repeat() {
         Node a = atom();
         for (;;) {
+            skip_space();
             int c = peek();
+            int lo, hi;
             if (c == '*') {
                 take();
-                a = rep(std::move(a), 0, -1);
+                lo = 0, hi = -1;
             } else if (c == '+') {
                 take();
-                a = rep(std::move(a), 1, -1);
+                lo = 1, hi = -1;
             } else if (c == '?') {
                 take();
-                a = rep(std::move(a), 0, 1);
+                lo = 0, hi = 1;
             } else if (c == '{') {
-                size_t j = s.find('}', i);
-                if (j == std::string::npos) throw Error{"bad repetition"};
-                std::string body = s.substr(i + 1, j - i - 1);
-                size_t comma = body.find(',');
-                std::string a_s = comma == std::string::npos ? body : body.substr(0, comma);
-                std::string b_s = comma == std::string::npos ? "" : body.substr(comma + 1);
-                auto digits = [](const std::string& t) {
-                    for (char ch : t)
-                        if (!is_digit(ch)) return false;
-                    return true;
-                };
-                if (a_s.empty() || !digits(a_s) || !digits(b_s) || a_s.size() > 4 || b_s.size() > 4)
-                    throw Error{"bad repetition"};
-                i = j + 1;
-                int lo = atoi(a_s.c_str());
-                int hi = comma == std::string::npos ? lo : (b_s.empty() ? -1 : atoi(b_s.c_str()));
-                if (hi >= 0 && hi < lo) throw Error{"bad repetition"};
-                a = rep(std::move(a), lo, hi);
+                take();
+                skip_space();
+                lo = decimal();
+                skip_space();
+                hi = lo;
+                if (peek() == ',') {
+                    take();
+                    skip_space();
+                    hi = peek() == '}' ? -1 : decimal();
+                    skip_space();
+                }
+                if (take() != '}') error("unclosed counted repetition");
+                if (hi >= 0 && hi < lo) error("invalid repetition range (min > max)");
             } else {
                 return a;
             }
+            skip_space();
+            if (peek() == '?') take();  // lazy: the same set of matches
+            a = rep(std::move(a), lo, hi);
         }
     }
-    u64 class_escape(int c) {
-        u64 m = 0;
-        if (c == 'd') {
-            for (int x = '0'; x <= '9'; x++) m |= 1ull << value_of(x);
-            return m;
-        }
-        if (c == 'w') {
-            for (int v = 0; v < 64; v++)
-                if (is_alpha(ALPHABET[v]) || is_digit(ALPHABET[v])) m |= 1ull << v;
-            return m;
-        }
-        return char_set(c, fold);
-    }
-    static Node set_node(u64 m) {
+    Node set_node(u64 m) {
         Node n;
         n.kind = Node::SET;
-        n.set = m;
+        n.set = f.i ? fold_set(m) : m;
         return n;
     }
+    static Node look_node(int k) {
+        Node n;
+        n.kind = Node::LOOK;
+        n.look = k;
+        return n;
+    }
+    Node word_look(int k) {
+        // the reference's DFA has no Unicode word boundary (regex-automata refuses it)
+        if (f.u) error("a Unicode word boundary is not supported (clear the u flag)");
+        return look_node(k);
+    }
+    // the value set of a Perl class letter (d D w W s S), or -1 when it is none
+    bool perl_class(int c, u64& m) {
+        switch (c) {
+            case 'd': m = range_set('0', '9'); return true;
+            case 'D': m = ~range_set('0', '9'); return true;
+            case 'w': m = WORD_VALUES; return true;  // [0-9A-Za-z_]: '_' is not base64
+            case 'W': m = ~WORD_VALUES; return true;
+            case 's': m = 0; return true;            // [\t\n\v\f\r ]: no base64 character
+            case 'S': m = ~0ull; return true;
+        }
+        return false;
+    }
+    int hex_digits(int n, bool braces) {
+        long v = 0;
+        int got = 0;
+        for (;;) {
+            int c = peek();
+            int d = is_digit(c) ? c - '0' : (c >= 'a' && c <= 'f') ? c - 'a' + 10 : (c >= 'A' && c <= 'F') ? c - 'A' + 10 : -1;
+            if (braces && c == '}') break;
+            if (d < 0) {
+                if (braces) error("invalid hexadecimal digit");
+                break;
+            }
+            take();
+            v = v * 16 + d;
+            if (v > 0x10ffff) error("hexadecimal escape out of range");
+            if (++got == n && !braces) break;
+        }
+        if (braces) {
+            if (take() != '}' || got == 0) error("invalid hexadecimal escape");
+        } else if (got != n) {
+            error("invalid hexadecimal escape");
+        }
+        return (int)v;
+    }
+    // a codepoint escape after the backslash (x, u, U, control letters or punctuation);
+    // -1 when `c` is not one
+    int literal_escape(int c) {
+        switch (c) {
+            case 'a': return 7;
+            case 'f': return 12;
+            case 't': return 9;
+            case 'n': return 10;
+            case 'r': return 13;
+            case 'v': return 11;
+            case 'x':
+                if (peek() == '{') { take(); return hex_digits(8, true); }
+                return hex_digits(2, false);
+            case 'u':
+                if (peek() == '{') { take(); return hex_digits(8, true); }
+                return hex_digits(4, false);
+            case 'U':
+                if (peek() == '{') { take(); return hex_digits(8, true); }
+                return hex_digits(8, false);
+        }
+        // superfluous escapes of ASCII punctuation (and of space) stand for the character
+        if (c >= 32 && c < 127 && !is_alnum(c) && c != '<' && c != '>') return c;
+        return -1;
+    }
+    [[noreturn]] void bad_escape(int c) {
+        if (c == 'p' || c == 'P') error("Unicode classes (\\p, \\P) are not supported");
+        if (is_digit(c)) error("backreferences are not supported");
+        error(std::string("unrecognized escape sequence '\\") + (char)c + "'");
+    }
+    u64 char_set(int c) { return value_of(c) >= 0 ? 1ull << value_of(c) : 0; }
+
+    Node escape() {
+        int c = take();
+        u64 m;
+        if (perl_class(c, m)) return set_node(m);
+        switch (c) {
+            case 'A': return look_node(L_START);
+            case 'z': return look_node(L_END);
+            case 'B': return word_look(L_NOT_WORD);
+            case '<': return word_look(L_WORD_START);
+            case '>': return word_look(L_WORD_END);
+            case 'b': {
+                if (peek() != '{') return word_look(L_WORD);
+                size_t j = s.find('}', i);
+                std::string name = j == std::string::npos ? "" : s.substr(i + 1, j - i - 1);
+                int k = name == "start" ? L_WORD_START : name == "end" ? L_WORD_END
+                      : name == "start-half" ? L_WORD_START_HALF : name == "end-half" ? L_WORD_END_HALF : 0;
+                if (!k) error("unrecognized special word boundary");
+                i = j + 1;
+                return word_look(k);
+            }
+        }
+        int cp = literal_escape(c);
+        if (cp < 0) bad_escape(c);
+        return set_node(char_set(cp));
+    }
+
+    // ---- bracketed classes ----
+    // one class item: a character (returned in *single when it may start a range) or a set
+    u64 class_atom(int* single) {
+        *single = -1;
+        int c = take();
+        if (c == '[') {
+            if (peek() == ':') {
+                size_t j = s.find(":]", i + 1);
+                if (j != std::string::npos) {
+                    std::string name = s.substr(i + 1, j - i - 1);
+                    bool neg = !name.empty() && name[0] == '^';
+                    if (neg) name.erase(0, 1);
+                    u64 m;
+                    if (posix_class(name, m)) {
+                        i = j + 2;
+                        return neg ? ~m : m;
+                    }
+                }
+            }
+            return bracket_body();  // nested class
+        }
+        if (c == '\\') {
+            int e = take();
+            u64 m;
+            if (perl_class(e, m)) return m;
+            int cp = literal_escape(e);
+            if (cp < 0) {
+                if (strchr("AzbB<>", e)) error("an assertion is not allowed in a character class");
+                bad_escape(e);
+            }
+            *single = cp;
+            return char_set(cp);
+        }
+        *single = c;
+        return char_set(c);
+    }
+    static bool posix_class(const std::string& n, u64& m) {
+        if (n == "alnum") m = range_set('0', '9') | range_set('A', 'Z') | range_set('a', 'z');
+        else if (n == "alpha") m = range_set('A', 'Z') | range_set('a', 'z');
+        else if (n == "ascii") m = ~0ull;
+        else if (n == "blank" || n == "cntrl" || n == "space") m = 0;
+        else if (n == "digit") m = range_set('0', '9');
+        else if (n == "graph" || n == "print") m = ~0ull;
+        else if (n == "lower") m = range_set('a', 'z');
+        else if (n == "punct") m = range_set('+', '+') | range_set('/', '/');
+        else if (n == "upper") m = range_set('A', 'Z');
+        else if (n == "word") m = WORD_VALUES;
+        else if (n == "xdigit") m = range_set('0', '9') | range_set('A', 'F') | range_set('a', 'f');
+        else return false;
+        return true;
+    }
+    // union of items up to ']' or a set operator (a range is x-y of two single characters)
+    u64 class_union(bool first) {
+        u64 m = 0;
+        bool any = false;
+        for (;;) {
+            skip_space();
+            int c = peek();
+            if (c < 0) error("unclosed character class");
+            if (c == ']' && !(first && !any)) break;
+            if ((c == '&' && peek_at(1) == '&') || (c == '-' && peek_at(1) == '-') || (c == '~' && peek_at(1) == '~'))
+                break;
+            int lo;
+            u64 item = class_atom(&lo);
+            any = true;
+            skip_space();
+            if (lo >= 0 && peek() == '-' && peek_at(1) != ']' && peek_at(1) != '-' && peek_at(1) >= 0) {
+                take();
+                skip_space();
+                int hi;
+                class_atom(&hi);
+                if (hi < 0) error("invalid range: the end is not a single character");
+                if (hi < lo) error("invalid range (start > end)");
+                item = range_set(lo, hi);
+            }
+            m |= f.i ? fold_set(item) : item;
+        }
+        if (!any && !first) error("empty operand of a class set operation");
+        return m;
+    }
+    // after '[': [^] items (op items)* ']'
+    u64 bracket_body() {
+        enter();
+        bool neg = false;
+        if (peek() == '^') {
+            take();
+            neg = true;
+        }
+        u64 m = class_union(true);
+        for (;;) {
+            int c = peek();
+            if (c == ']') {
+                take();
+                break;
+            }
+            int op = take();
+            take();  // the second character of &&, --, ~~
+            u64 r = class_union(false);
+            m = op == '&' ? (m & r) : op == '-' ? (m & ~r) : (m ^ r);
+        }
+        depth--;
+        return neg ? ~m : m;
+    }
+
     Node atom() {
         int c = take();
         if (c == '(') {
-            if (s.compare(i, 2, "?:") == 0) i += 2;
+            Flags saved = f;
+            if (peek() == '?') {
+                take();
+                if (peek() == 'P' && peek_at(1) == '<') {
+                    i += 2;
+                    group_name();
+                } else if (peek() == '<') {
+                    take();
+                    group_name();
+                } else {
+                    parse_flags(':');
+                }
+            }
             Node n = alt();
-            if (take() != ')') throw Error{"unclosed group"};
+            f = saved;
+            if (eof() || take() != ')') error("unclosed group");
             return n;
         }
         if (c == '.') return set_node(~0ull);
-        if (c == '^') {
-            Node n;
-            n.kind = Node::BOL;
-            return n;
-        }
-        if (c == '$') {
-            Node n;
-            n.kind = Node::EOL;
-            return n;
-        }
-        if (c == '\\') return set_node(class_escape(take()));
+        if (c == '^') return look_node(L_START);
+        if (c == '$') return look_node(L_END);
+        if (c == '\\') return escape();
         if (c == '[') {
-            bool neg = false;
-            if (peek() == '^') {
-                take();
-                neg = true;
-            }
-            u64 m = 0;
-            bool first = true;
-            for (;;) {
-                int ch = take();
-                if (ch == ']' && !first) break;
-                first = false;
-                if (ch == '\\') {
-                    m |= class_escape(take());
-                    continue;
-                }
-                if (peek() == '-' && i + 1 < s.size() && s[i + 1] != ']') {
-                    take();
-                    int hi = take();
-                    for (int x = ch; x <= hi; x++) m |= char_set(x, fold);
-                } else {
-                    m |= char_set(ch, fold);
-                }
-            }
-            return set_node(neg ? ~m : m);
+            u64 m = bracket_body();
+            Node n;
+            n.kind = Node::SET;
+            n.set = m;  // folding was applied item by item, before any negation
+            return n;
         }
-        if (c == '*' || c == '+' || c == '?' || c == '{') throw Error{"repetition without operand"};
-        return set_node(char_set(c, fold));
+        if (c == '*' || c == '+' || c == '?' || c == '{') error("repetition operator missing expression");
+        if (c == ')') error("unopened group");
+        return set_node(char_set(c));
+    }
+    void group_name() {
+        size_t j = s.find('>', i);
+        if (j == std::string::npos || j == i) error("invalid capture group name");
+        for (size_t k = i; k < j; k++) {
+            int ch = (unsigned char)s[k];
+            bool ok = is_alnum(ch) || ch == '_' || ((ch == '.' || ch == '[' || ch == ']') && k > i);
+            if (!ok || (k == i && is_digit(ch))) error("invalid capture group name");
+        }
+        i = j + 1;
     }
 };
 
 int min_len(const Node& n) {
     switch (n.kind) {
         case Node::SET: return 1;
-        case Node::BOL:
-        case Node::EOL: return 0;
+        case Node::LOOK: return 0;
         case Node::CAT: {
             int t = 0;
             for (auto& k : n.kids) t += min_len(k);
@@ -238,12 +548,31 @@ int min_len(const Node& n) {
     return 0;
 }
 
+// Where an assertion is evaluated: the haystack position and its neighbours.
+struct At {
+    bool start, end, prev_word, next_word;
+};
+
+bool look_holds(int k, const At& a) {
+    switch (k) {
+        case L_START: return a.start;
+        case L_END: return a.end;
+        case L_WORD: return a.prev_word != a.next_word;
+        case L_NOT_WORD: return a.prev_word == a.next_word;
+        case L_WORD_START: return !a.prev_word && a.next_word;
+        case L_WORD_END: return a.prev_word && !a.next_word;
+        case L_WORD_START_HALF: return !a.prev_word;
+        case L_WORD_END_HALF: return !a.next_word;
+    }
+    return false;
+}
+
 struct Nfa {
-    enum { PLAIN = 0, BOL = 1, EOL = 2 };
-    std::vector<std::vector<std::pair<int, int>>> eps;  // (kind, target)
+    std::vector<std::vector<std::pair<int, int>>> eps;  // (0 plain or a Look kind, target)
     std::vector<u64> sym;                                // symbol set of the state's edge
     std::vector<int> sym_to;                             // its target, -1 for none
-    size_t limit;
+    size_t limit = 1u << 20;
+    bool has_start = false, has_word = false;
 
     int add() {
         if (eps.size() >= limit) throw Error{"pattern too large"};
@@ -258,8 +587,11 @@ struct Nfa {
                 sym[a] = n.set;
                 sym_to[a] = b;
                 break;
-            case Node::BOL: eps[a].push_back({BOL, b}); break;
-            case Node::EOL: eps[a].push_back({EOL, b}); break;
+            case Node::LOOK:
+                eps[a].push_back({n.look, b});
+                if (n.look == L_START) has_start = true;
+                if (is_word_look(n.look)) has_word = true;
+                break;
             case Node::CAT: {
                 int cur = a;
                 for (auto& k : n.kids) {
@@ -267,15 +599,15 @@ struct Nfa {
                     build(k, cur, nxt);
                     cur = nxt;
                 }
-                eps[cur].push_back({PLAIN, b});
+                eps[cur].push_back({0, b});
                 break;
             }
             case Node::ALT:
                 for (auto& k : n.kids) {
                     int x = add(), y = add();
-                    eps[a].push_back({PLAIN, x});
+                    eps[a].push_back({0, x});
                     build(k, x, y);
-                    eps[y].push_back({PLAIN, b});
+                    eps[y].push_back({0, b});
                 }
                 break;
             case Node::REP: {
@@ -288,17 +620,17 @@ struct Nfa {
                 }
                 if (n.hi < 0) {
                     int x = add(), y = add();
-                    eps[cur].push_back({PLAIN, x});
+                    eps[cur].push_back({0, x});
                     build(sub, x, y);
-                    eps[y].push_back({PLAIN, x});
-                    eps[x].push_back({PLAIN, b});
-                    eps[cur].push_back({PLAIN, b});
+                    eps[y].push_back({0, x});
+                    eps[x].push_back({0, b});
+                    eps[cur].push_back({0, b});
                 } else {
-                    eps[cur].push_back({PLAIN, b});
+                    eps[cur].push_back({0, b});
                     for (int k = 0; k < n.hi - n.lo; k++) {
                         int nxt = add();
                         build(sub, cur, nxt);
-                        eps[nxt].push_back({PLAIN, b});
+                        eps[nxt].push_back({0, b});
                         cur = nxt;
                     }
                 }
@@ -306,21 +638,59 @@ struct Nfa {
             }
         }
     }
-    std::set<int> closure(const std::set<int>& states, bool at_start, bool at_end) const {
-        std::set<int> out(states);
-        std::vector<int> stack(states.begin(), states.end());
+    // Closure of `states` (sorted, unique) over plain edges and the assertions that hold at
+    // `at`; `decided` = false leaves the word assertions and the end assertion unfollowed
+    // (their next character is not known yet).
+    std::vector<int> closure(const std::vector<int>& states, const At& at, bool decided, std::vector<int>& mark,
+                             int& stamp) const {
+        stamp++;
+        std::vector<int> out, stack;
+        for (int s : states)
+            if (mark[s] != stamp) {
+                mark[s] = stamp;
+                stack.push_back(s);
+            }
         while (!stack.empty()) {
             int s = stack.back();
             stack.pop_back();
+            out.push_back(s);
             for (auto& e : eps[s]) {
-                if (e.first == BOL && !at_start) continue;
-                if (e.first == EOL && !at_end) continue;
-                if (out.insert(e.second).second) stack.push_back(e.second);
+                if (e.first != 0) {
+                    const bool known = e.first == L_START || decided;
+                    if (!known || !look_holds(e.first, at)) continue;
+                }
+                if (mark[e.second] != stamp) {
+                    mark[e.second] = stamp;
+                    stack.push_back(e.second);
+                }
             }
         }
+        std::sort(out.begin(), out.end());
         return out;
     }
 };
+
+// Probability that a uniformly random key matches the table (the first searched character
+// takes 16 values, the others 64), propagated character by character.
+double table_probability(const std::vector<std::vector<uint32_t>>& trans, const std::vector<bool>& eoi) {
+    const size_t n = trans.size();
+    std::vector<double> d(n, 0.0), nd(n);
+    d[1] = 1.0;
+    for (int pos = 0; pos < 43; pos++) {
+        std::fill(nd.begin(), nd.end(), 0.0);
+        const int values = pos == 0 ? 16 : 64;
+        for (size_t s = 0; s < n; s++) {
+            if (d[s] == 0.0) continue;
+            const double w = d[s] / values;
+            for (int v = 0; v < values; v++) nd[trans[s][v]] += w;
+        }
+        d.swap(nd);
+    }
+    double p = 0;
+    for (size_t s = 0; s < n; s++)
+        if (s == 0 || eoi[s]) p += d[s];
+    return p;
+}
 
 }  // namespace
 
@@ -335,47 +705,77 @@ extern "C" int mk_regex_compile(const char* pattern, int case_sensitive, uint32_
     *states = 0;
     try {
         std::string s(pattern);
+        if (s.empty()) return error("the pattern is empty", MK_ERR_PATTERN);
         Parser p(s, case_sensitive == 0);
         Node ast = p.parse();
         if (min_len(ast) == 0) return error("the pattern matches the empty string", MK_ERR_PATTERN);
         Nfa nfa;
-        nfa.limit = 1u << 20;
         int start = nfa.add(), match = nfa.add();
         nfa.build(ast, start, match);
-        std::map<std::set<int>, uint32_t> ids;
-        std::vector<std::set<int>> order;
+        std::vector<int> mark(nfa.eps.size(), 0);
+        int stamp = 0;
+        // a DFA state: NFA states (closed over plain edges and the start assertion where it
+        // holds), whether the previous character was a word character (kept only when the
+        // pattern has word assertions), and whether nothing has been read yet (kept only when
+        // start assertions can be reached through word assertions)
+        typedef std::tuple<std::vector<int>, int, int> Key;
+        const bool track_word = nfa.has_word, track_start = nfa.has_word && nfa.has_start;
+        std::map<Key, uint32_t> ids;
+        std::vector<Key> order;
         std::vector<std::vector<uint32_t>> trans(1, std::vector<uint32_t>(64, 0));  // state 0: accept
         std::vector<bool> eoi(1, true);
-        std::set<int> s0 = nfa.closure({start}, true, false);
-        ids[s0] = 1;
-        order.push_back(s0);
+        const At at0{true, false, false, false};
+        Key k0{nfa.closure({start}, at0, false, mark, stamp), 0, track_start ? 1 : 0};
+        ids[k0] = 1;
+        order.push_back(k0);
         for (size_t k = 0; k < order.size(); k++) {
-            const std::set<int> S = order[k];
+            const std::vector<int> S = std::get<0>(order[k]);
+            const bool prev_word = std::get<1>(order[k]) != 0;
+            const bool first = k == 0;  // only the start state has read nothing
             std::vector<uint32_t> row(64);
             for (int v = 0; v < 64; v++) {
-                std::set<int> nxt;
-                for (int st : S)
-                    if (nfa.sym_to[st] >= 0 && ((nfa.sym[st] >> v) & 1)) nxt.insert(nfa.sym_to[st]);
-                nxt.insert(start);  // unanchored: a match may start after this character
-                std::set<int> T = nfa.closure(nxt, false, false);
-                if (T.count(match)) {
+                const bool w = value_is_word(v);
+                // assertions between the previous character and this one
+                const std::vector<int> C = track_word ? nfa.closure(S, At{first, false, prev_word, w}, true, mark, stamp) : S;
+                if (std::binary_search(C.begin(), C.end(), match)) {
                     row[v] = 0;
                     continue;
                 }
-                auto it = ids.find(T);
+                std::vector<int> nxt;
+                for (int st : C)
+                    if (nfa.sym_to[st] >= 0 && ((nfa.sym[st] >> v) & 1)) nxt.push_back(nfa.sym_to[st]);
+                nxt.push_back(start);  // unanchored: a match may start after this character
+                std::sort(nxt.begin(), nxt.end());
+                nxt.erase(std::unique(nxt.begin(), nxt.end()), nxt.end());
+                std::vector<int> T = nfa.closure(nxt, At{false, false, w, false}, false, mark, stamp);
+                if (std::binary_search(T.begin(), T.end(), match)) {
+                    row[v] = 0;
+                    continue;
+                }
+                Key key{std::move(T), track_word && w ? 1 : 0, 0};
+                auto it = ids.find(key);
                 if (it == ids.end()) {
                     uint32_t id = (uint32_t)order.size() + 1;
-                    ids[T] = id;
-                    order.push_back(T);
-                    if (order.size() + 1 > max_states) return error("the DFA has too many states", MK_ERR_PATTERN);
+                    if (order.size() + 2 > max_states)
+                        return error("the regular expression is too complex (the DFA has more than " +
+                                         std::to_string(max_states) + " states)",
+                                     MK_ERR_PATTERN);
+                    ids[key] = id;
+                    order.push_back(key);
                     row[v] = id;
                 } else {
                     row[v] = it->second;
                 }
             }
             trans.push_back(row);
-            eoi.push_back(S.count(match) || nfa.closure(S, false, true).count(match));
+            // end of input: no character follows
+            const std::vector<int> E = nfa.closure(S, At{first, true, prev_word, false}, true, mark, stamp);
+            eoi.push_back(std::binary_search(E.begin(), E.end(), match));
         }
+        if (table_probability(trans, eoi) == 0.0)
+            return error("no public key matches this regular expression (the characters are A-Z a-z 0-9 + /, "
+                         "and the one right after the fixed part is A-P)",
+                         MK_ERR_PATTERN);
         const size_t n = trans.size();
         for (size_t st = 0; st < n; st++) {
             for (int v = 0; v < 65; v++) {

@@ -45,8 +45,9 @@ class Needle:
         return Needle(bytes(table), L.MODE_REGEX, False, states)
 
     @staticmethod
-    def regex(pattern: str, case_sensitive: bool = True, max_states: int = 4096) -> "Needle":
-        """A regex needle compiled by the library (mk_regex_compile)."""
+    def regex(pattern: str, case_sensitive: bool = True, max_states: int = 16384) -> "Needle":
+        """A regex needle compiled by the library (mk_regex_compile); max_states defaults to the
+        reference's limit (MAX_STATES, src/model/pattern/dfa.rs:18)."""
         lib = L.load()
         table = ctypes.create_string_buffer(max_states * 130)
         states = ctypes.c_uint32()

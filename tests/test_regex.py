@@ -13,7 +13,7 @@ import meikey_b200 as mk
 PATTERNS = [
     ("ab", True), ("[0-9]$", True), ("^[A-P]a", True), ("wa.o", False), ("(ab){2,}", True),
     ("zzzz|ofX", True), ("[0-9][A-F]x", False), ("a+b/c?", True), ("^[^A]", True), ("9$", True),
-    ("\\d\\w{2}", True), ("(?:xy|z+)[+/]{1,3}$", False), ("^a.{3}b", True), ("[]a]", True), ("[a-]", True),
+    ("\\d\\w{2}", True), ("(?:xy|z+)[+/]{1,3}$", False), ("^A.{3}b", True), ("[]a]", True), ("[a-]", True),
     ("q{2}", True), ("(a|b|c)(d|e)", False), ("[^0-9a-z]{4}", True), ("K\\+", True), ("(x(y(z)?)?)w", True),
 ]
 
@@ -64,5 +64,8 @@ def test_expected_tries_exact():
     # first character from 16 values that cannot be 'z')
     e1 = mk.Needle.contains("z").expected_tries()
     assert abs(1 / e1 - (1 - (63 / 64) ** 42)) < 1e-12
-    # a regex that cannot match at the first position ('a' is not among its 16 values)
-    assert mk.Needle.regex("^a").expected_tries() == float("inf")
+    # a regex that no key can match ('a' is not among the 16 values of the first position) is
+    # refused at compile time, as the reference's Pattern::regex refuses it (NeverMatches)
+    with pytest.raises(mk.GpuError) as e:
+        mk.Needle.regex("^a")
+    assert e.value.status == mk._lib.ERR_PATTERN and "no public key matches" in str(e.value)
