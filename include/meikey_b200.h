@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define MK_ABI_VERSION 1
+#define MK_ABI_VERSION 2
 
 #if defined(__GNUC__)
 #define MK_API __attribute__((visibility("default")))
@@ -154,6 +154,9 @@ typedef struct mk_server_options {
     uint32_t iters_per_tick; /* iterations per tick (one launch of iters_per_tick·keys_per_iter indices) */
     uint64_t budget;         /* indices a job searches from its admission before it is censored */
     uint64_t hit_capacity;   /* hit-ring entries the admitted jobs may plan for (0 = no limit) */
+    uint64_t device_bytes;   /* device memory the admitted jobs may hold (0 = no limit): per job its
+                                reserved hit-ring records (16 bytes each; four times its expected
+                                candidates per tick, plus 64), its DFA table and 64 bytes of state */
 } mk_server_options;
 
 /* A finished job of the server. */
@@ -233,7 +236,11 @@ MK_API int mk_job_stop(mk_job* job, int on);
 /* For each needle k < n: the lowest candidate of the last launch (or graph replay) that the
  * host confirms (mk_job_confirm, in index order), in out[k] (status MK_OK with index, key and
  * secret; MK_ERR_STOPPED when none of its candidates matches with the real x sign).  Needles
- * are confirmed on up to 16 host threads of the call's own; it returns when all are done. */
+ * are confirmed on up to 16 host threads of the call's own (fewer, down to the calling thread
+ * alone, when the host starts no more); it returns when all are done.  When the launch found
+ * more candidates than the hit ring holds, the outcomes are those of the kept candidates, which
+ * need not include a needle's lowest one, and MK_ERR_HIT_RING_FULL is returned (as by
+ * mk_job_hits; launch fewer iterations or raise mk_options.hit_capacity). */
 MK_API int mk_job_first_matches(mk_job* job, mk_outcome* out, uint32_t n);
 
 /* Validates needles as mk_job_prepare would (host only, no device). */
@@ -263,11 +270,14 @@ MK_API int mk_search(mk_job* job, const mk_search_config* cfg, mk_progress_fn pr
  * reference): every mk_server_tick is one launch over the next iters_per_tick·keys_per_iter
  * indices of the stream (key, seed source) that tests the needles of all admitted jobs.
  * Submitted jobs wait in a queue and are admitted at tick boundaries, shortest expected
- * search first, while needle slots, the matcher's capacity and the hit-ring plan allow.
- * A job admitted at stream index a searches [a, a + budget): its result is the lowest index
- * there whose key matches (confirmed on the host), the same key mk_search finds for that
- * needle alone from first = a; otherwise it is censored at the budget.  The server keeps a
- * job of its own on the context; ticks are synchronous. */
+ * search first, while needle slots, the matcher's capacity, the hit-ring plan and the
+ * device-memory budget allow.  A job admitted at stream index a searches [a, a + budget):
+ * its result is the lowest index there whose key matches (confirmed on the host) and that
+ * no other job has received: one index, so one secret, goes to one job only; of two jobs
+ * matching the same key the one admitted earlier gets it.  That is the key mk_search finds
+ * for the needle alone from first = a once the indices delivered before it (in the order
+ * mk_server_results returns them) are skipped; otherwise the job is censored at the budget.
+ * The server keeps a job of its own on the context; ticks are synchronous. */
 MK_API int mk_server_create(mk_ctx* ctx, const uint8_t key[32], int seed_source, const mk_server_options* options,
                             uint64_t first, mk_server** out);
 MK_API int mk_server_submit(mk_server* server, const mk_needle* needle, uint64_t id);
@@ -307,20 +317,30 @@ MK_API int mk_derive(mk_ctx* ctx, const uint8_t key[32], int seed_source, uint64
  * synchronize the device and stall every other job sharing it.  The device staging for the
  * keys is a fixed 2 MiB array inside the library (held by every GPU that loads it until the
  * process exits), so n is limited to 65536 keys; larger n returns MK_ERR_OUT_OF_RANGE.
- * The first call on a device looks the array's device address up (make that first call
- * before any stream capture).  All calls share the array: calls that overlap on the GPU,
- * from any thread or context on the same device, race on it. */
+ * Seed sources MK_SEED_CHACHA20 and MK_SEED_COUNTER only: MK_SEED_INCREMENTAL returns
+ * MK_ERR_BAD_ARG (use mk_derive).  The array's device address is looked up by mk_ctx_create,
+ * with the context's device current, and kept in the context; a cudaDeviceReset of that device
+ * invalidates it together with the context's other device memory, so create a new context
+ * after one.  All calls share the array: calls that overlap on the GPU, from any thread or
+ * context on the same device, race on it. */
 MK_API int mk_derive_noalloc(mk_ctx* ctx, const uint8_t key[32], int seed_source, uint64_t first, uint64_t n,
                              uint8_t* out);
 
-/* Dfa::new + Dfa::gpu_table (src/model/pattern/dfa.rs:52-108, 189-200): compiles a regex
- * into the DFA table of a MK_MODE_REGEX needle (states × 65 little-endian u16, state 0
- * accepts, state 1 starts, column 64 flags acceptance at the end), for an unanchored search
- * over the 43 characters after the key prefix.  Syntax: literals, `.`, classes with ranges
- * and negation, \d, \w, escapes, groups, `|`, `*`, `+`, `?`, `{m}`, `{m,}`, `{m,n}`, `^`,
- * `$`; case_sensitive = 0 matches letters in both cases.  `table` must hold
- * max_states·130 bytes.  Returns MK_ERR_PATTERN (text in `err`) for a syntax error, a pattern
- * that matches the empty string, or more than max_states states.  Needs no device. */
+/* Dfa::new + Dfa::gpu_table with the checks of Pattern::regex (src/model/pattern/dfa.rs:52-108,
+ * 189-200; src/model/pattern.rs:135-165): compiles a regex into the DFA table of a
+ * MK_MODE_REGEX needle (states × 65 little-endian u16, state 0 accepts, state 1 starts,
+ * column 64 flags acceptance at the end), for an unanchored search over the 43 characters
+ * after the key prefix, which form the whole haystack.  The dialect is the reference's:
+ * regex-syntax in ASCII mode (literals, `.`, classes with ranges, negation, nesting, POSIX
+ * names and the && -- ~~ operations, \d \D \w \W \s \S, ^ $ \A \z \b \B \< \> \b{start}
+ * \b{end} \b{start-half} \b{end-half}, punctuation / control / hex escapes, groups incl. named
+ * ones, flag groups (?imsUuxR-...) and (?flags:...), `|`, * + ? {m} {m,} {m,n} and their lazy
+ * forms); case_sensitive = 0 starts with the i flag set.  Unicode classes (\p, \P) and a
+ * Unicode word boundary (\b under the u flag) are rejected, as is every escape outside the
+ * dialect.  `table` must hold max_states·130 bytes (the reference's limit is 16384 states).
+ * Returns MK_ERR_PATTERN (text in `err`) for an empty pattern, a syntax error, a pattern
+ * that matches the empty string, one that no public key can match (e.g. `^Q`: the first
+ * searched character is A-P) or more than max_states states.  Needs no device. */
 MK_API int mk_regex_compile(const char* pattern, int case_sensitive, uint32_t max_states, uint8_t* table,
                             uint32_t* states, char* err, size_t err_size);
 

@@ -70,7 +70,7 @@ class OutcomeC(ctypes.Structure):
 
 class ServerOptionsC(ctypes.Structure):
     _fields_ = [("max_jobs", ctypes.c_uint32), ("iters_per_tick", ctypes.c_uint32), ("budget", ctypes.c_uint64),
-                ("hit_capacity", ctypes.c_uint64)]
+                ("hit_capacity", ctypes.c_uint64), ("device_bytes", ctypes.c_uint64)]
 
 
 class JobResultC(ctypes.Structure):

@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "../../include/meikey_b200.h"
+#include "abi_guard.h"
 #include "hitsort.h"
 #include "host25519.h"
 #include "kernels.h"
@@ -40,6 +41,7 @@ struct mk_ctx {
     uint32_t hash_warps = 0;  // 4: search kernel with hashing warps (ChaCha20 / counter seeds)
     uint32_t layout = mkb::LAYOUT_INVERTER_WARP;  // division of work inside a search CTA
     uint32_t hit_capacity = 1u << 16;
+    uint8_t* noalloc = nullptr;  // device address of mk_derive_noalloc's fixed staging array
     std::string err;
 };
 
@@ -221,7 +223,7 @@ int mk_last_error(const mk_ctx* ctx, char* buf, size_t size) {
     return MK_OK;
 }
 
-int mk_ctx_create(int device, const mk_options* options, mk_ctx** out) {
+int mk_ctx_create(int device, const mk_options* options, mk_ctx** out) try {
     if (!out) return MK_ERR_BAD_ARG;
     *out = nullptr;
     int n = 0;
@@ -251,6 +253,7 @@ int mk_ctx_create(int device, const mk_options* options, mk_ctx** out) {
     c->layout = o.hash_warps ? mkb::LAYOUT_HASH_WARPS : o.inverter_rotates ? mkb::LAYOUT_ROTATING : mkb::LAYOUT_INVERTER_WARP;
     if (o.hit_capacity) c->hit_capacity = o.hit_capacity;
     MK_CUDA(c, cudaSetDevice(device));
+    MK_CUDA(c, mkb::noalloc_staging(&c->noalloc));
     MK_CUDA(c, cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     MK_CUDA(c, cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
     {
@@ -323,9 +326,9 @@ int mk_ctx_create(int device, const mk_options* options, mk_ctx** out) {
         if (st) return st;
     }
     return MK_OK;
-}
+} MK_ABI_CATCH(out && *out ? &(*out)->err : nullptr)
 
-void mk_ctx_destroy(mk_ctx* c) {
+void mk_ctx_destroy(mk_ctx* c) try {
     if (!c) return;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
@@ -337,7 +340,7 @@ void mk_ctx_destroy(mk_ctx* c) {
     if (c->stream) cudaStreamDestroy(c->stream);
     if (c->pool) cudaMemPoolDestroy(c->pool);
     delete c;
-}
+} MK_ABI_CATCH_VOID
 
 int mk_ctx_info(const mk_ctx* c, mk_info* out) {
     if (!c || !out) return MK_ERR_BAD_ARG;
@@ -355,7 +358,7 @@ static int check_source(mk_ctx* c, const uint8_t key[32], int seed_source) {
     return MK_OK;
 }
 
-int mk_derive(mk_ctx* c, const uint8_t key[32], int seed_source, uint64_t first, uint64_t n, uint8_t* out) {
+int mk_derive(mk_ctx* c, const uint8_t key[32], int seed_source, uint64_t first, uint64_t n, uint8_t* out) try {
     if (!c || !key || (!out && n)) return fail(c, MK_ERR_BAD_ARG, "bad argument");
     if (int st = check_source(c, key, seed_source)) return st;
     if (seed_source == MK_SEED_INCREMENTAL && n != 0 && n - 1 > ~0ull - first)  // last index first + n - 1
@@ -390,19 +393,20 @@ int mk_derive(mk_ctx* c, const uint8_t key[32], int seed_source, uint64_t first,
     }
     cudaFree(d_out);
     return MK_OK;
-}
+} MK_ABI_CATCH(c ? &c->err : nullptr)
 
 // Same keys as mk_derive, with the device output staged in the library's fixed device
 // array instead of a cudaMalloc'd buffer: this call allocates nothing.  Every slot of the
 // staging that is copied back is written by the kernel first, so nothing has to be cleared.
-int mk_derive_noalloc(mk_ctx* c, const uint8_t key[32], int seed_source, uint64_t first, uint64_t n, uint8_t* out) {
-    if (!c || !key || (!out && n) || (seed_source != 0 && seed_source != 1)) return fail(c, MK_ERR_BAD_ARG, "bad argument");
+int mk_derive_noalloc(mk_ctx* c, const uint8_t key[32], int seed_source, uint64_t first, uint64_t n, uint8_t* out) try {
+    if (!c || !key || (!out && n)) return fail(c, MK_ERR_BAD_ARG, "bad argument");
+    if (seed_source != MK_SEED_CHACHA20 && seed_source != MK_SEED_COUNTER)
+        return fail(c, MK_ERR_BAD_ARG, "mk_derive_noalloc: ChaCha20 and counter seeds only (use mk_derive)");
     if (n > mkb::NOALLOC_MAX_KEYS)
         return fail(c, MK_ERR_OUT_OF_RANGE, "mk_derive_noalloc: n exceeds the fixed staging of 65536 keys");
     if (n == 0) return MK_OK;
     MK_CUDA(c, cudaSetDevice(c->device));
-    uint8_t* staging = nullptr;
-    MK_CUDA(c, mkb::noalloc_staging(c->device, &staging));
+    uint8_t* staging = c->noalloc;
     mkb::KeyLaunch L{};
     L.table = c->table;
     L.geom = c->geom;
@@ -419,7 +423,7 @@ int mk_derive_noalloc(mk_ctx* c, const uint8_t key[32], int seed_source, uint64_
     MK_CUDA(c, cudaMemcpyAsync(out, staging, n * 32, cudaMemcpyDeviceToHost, c->stream));
     MK_CUDA(c, cudaStreamSynchronize(c->stream));
     return MK_OK;
-}
+} MK_ABI_CATCH(c ? &c->err : nullptr)
 
 int mk_table_entry(mk_ctx* c, uint32_t row, uint64_t col, uint32_t out[24]) {
     if (!c || !out || row >= c->geom.rows || col >= c->geom.cols[row]) return fail(c, MK_ERR_BAD_ARG, "bad table entry");
@@ -589,7 +593,7 @@ static int upload_needles(mk_job* j, mkb::MatchSet& ms, std::vector<mkh25519::Ne
 }
 
 int mk_job_prepare(mk_ctx* c, const uint8_t key[32], int seed_source, const mk_needle* needles, uint32_t n_needles,
-                   int stop_on_hit, mk_job** out) {
+                   int stop_on_hit, mk_job** out) try {
     if (!c || !key || !out || (n_needles && !needles)) return fail(c, MK_ERR_BAD_ARG, "bad argument");
     if (int st = check_source(c, key, seed_source)) return st;
     if (seed_source == MK_SEED_INCREMENTAL && c->hash_warps)
@@ -630,18 +634,18 @@ int mk_job_prepare(mk_ctx* c, const uint8_t key[32], int seed_source, const mk_n
     if (cudaStreamSynchronize(c->stream) != cudaSuccess) return bail(MK_ERR_CUDA, "job buffers");
     *out = j;
     return MK_OK;
-}
+} MK_ABI_CATCH(c ? &c->err : nullptr)
 
-int mk_needles_check(const mk_needle* needles, uint32_t n_needles) {
+int mk_needles_check(const mk_needle* needles, uint32_t n_needles) try {
     std::unique_ptr<mkb::MatchSet> ms(new (std::nothrow) mkb::MatchSet);
     if (!ms) return MK_ERR_OUT_OF_MEMORY;
     std::vector<mkh25519::Needle> hosts;
     return pack_needles(nullptr, needles, n_needles, *ms, hosts, nullptr);
-}
+} MK_ABI_CATCH(nullptr)
 
 uint64_t mk_job_keys_per_iter(const mk_job* j) { return j && j->ctx ? j->ctx->info.keys_per_iter : 0; }
 
-int mk_job_update(mk_job* j, const mk_needle* needles, uint32_t n_needles) {
+int mk_job_update(mk_job* j, const mk_needle* needles, uint32_t n_needles) try {
     if (!j) return MK_ERR_BAD_ARG;
     mk_ctx* c = j->ctx;
     MK_CUDA(c, cudaSetDevice(c->device));
@@ -651,9 +655,9 @@ int mk_job_update(mk_job* j, const mk_needle* needles, uint32_t n_needles) {
     std::vector<uint32_t> gram4;
     if (int st = pack_needles(c, needles, n_needles, *ms, hosts, &gram4)) return st;
     return upload_needles(j, *ms, hosts, gram4);
-}
+} MK_ABI_CATCH(j && j->ctx ? &j->ctx->err : nullptr)
 
-void mk_job_destroy(mk_job* j) {
+void mk_job_destroy(mk_job* j) try {
     if (!j) return;
     if (j->ctx) cudaSetDevice(j->ctx->device);
     if (j->ctx && j->ctx->stream) {
@@ -672,7 +676,7 @@ void mk_job_destroy(mk_job* j) {
         }
     }
     delete j;
-}
+} MK_ABI_CATCH_VOID
 
 // Shared memory for the job's DFA tables when they fit (the kernel then reads them there).
 static uint32_t dfa_smem_bytes(const mk_job* j) {
@@ -722,11 +726,11 @@ static int enqueue(mk_job* j, uint64_t base, uint32_t iters) {
     return MK_OK;
 }
 
-int mk_job_enqueue(mk_job* j, uint64_t base, uint32_t iters) {
+int mk_job_enqueue(mk_job* j, uint64_t base, uint32_t iters) try {
     if (!j) return MK_ERR_BAD_ARG;
     if (iters == 0) return MK_OK;
     return enqueue(j, base, iters);
-}
+} MK_ABI_CATCH(j && j->ctx ? &j->ctx->err : nullptr)
 
 // Waits for the job's queued work, then reads its state and hit ring (sorted by index).
 static int collect(mk_job* j, int* found, uint64_t* index) {
@@ -758,16 +762,16 @@ static int collect(mk_job* j, int* found, uint64_t* index) {
     return MK_OK;
 }
 
-int mk_job_collect(mk_job* j, int* found, uint64_t* index) {
+int mk_job_collect(mk_job* j, int* found, uint64_t* index) try {
     if (!j) return MK_ERR_BAD_ARG;
     j->last.clear();
     j->last_total = 0;
     if (found) *found = 0;
     MK_CUDA(j->ctx, cudaSetDevice(j->ctx->device));
     return collect(j, found, index);
-}
+} MK_ABI_CATCH(j && j->ctx ? &j->ctx->err : nullptr)
 
-int mk_job_launch(mk_job* j, uint64_t base, uint32_t iters, int* found, uint64_t* index) {
+int mk_job_launch(mk_job* j, uint64_t base, uint32_t iters, int* found, uint64_t* index) try {
     if (!j) return MK_ERR_BAD_ARG;
     j->last.clear();
     j->last_total = 0;
@@ -776,9 +780,9 @@ int mk_job_launch(mk_job* j, uint64_t base, uint32_t iters, int* found, uint64_t
     int st = enqueue(j, base, iters);
     if (st) return st;
     return collect(j, found, index);
-}
+} MK_ABI_CATCH(j && j->ctx ? &j->ctx->err : nullptr)
 
-int mk_job_hits(mk_job* j, mk_hit* out, uint32_t cap, uint32_t* written, uint64_t* total) {
+int mk_job_hits(mk_job* j, mk_hit* out, uint32_t cap, uint32_t* written, uint64_t* total) try {
     if (!j || !written || !total || (cap && !out)) return MK_ERR_BAD_ARG;
     *total = j->last_total;
     uint32_t k = std::min<uint32_t>(cap, (uint32_t)j->last.n);
@@ -789,7 +793,7 @@ int mk_job_hits(mk_job* j, mk_hit* out, uint32_t cap, uint32_t* written, uint64_
     if (k) memcpy(out, j->last.data(), sizeof(mk_hit) * k);
     *written = k;
     return j->last_total > j->cap ? MK_ERR_HIT_RING_FULL : MK_OK;
-}
+} MK_ABI_CATCH(j && j->ctx ? &j->ctx->err : nullptr)
 
 // Re-derives a candidate on the host and tests its needle with the real x sign.  Touches no
 // shared state (host threads confirm different needles at once); 1 / 2 for a bad needle or
@@ -814,11 +818,11 @@ static int confirm_fail(mk_job* j, int e) {
                 e == 1 ? "needle index out of range" : "incremental start scalar must be below 2^255");
 }
 
-int mk_job_confirm(mk_job* j, uint64_t index, uint32_t needle, uint8_t pk[32], uint8_t secret[32], int* matched) {
+int mk_job_confirm(mk_job* j, uint64_t index, uint32_t needle, uint8_t pk[32], uint8_t secret[32], int* matched) try {
     if (!j || !pk || !secret || !matched) return MK_ERR_BAD_ARG;
     if (int e = confirm_key(j, index, needle, pk, secret, matched)) return confirm_fail(j, e);
     return MK_OK;
-}
+} MK_ABI_CATCH(j && j->ctx ? &j->ctx->err : nullptr)
 
 int mk_job_stop(mk_job* j, int on) {
     if (!j) return MK_ERR_BAD_ARG;
@@ -831,7 +835,7 @@ int mk_job_stop(mk_job* j, int on) {
     return MK_OK;
 }
 
-int mk_job_first_matches(mk_job* j, mk_outcome* out, uint32_t n) {
+int mk_job_first_matches(mk_job* j, mk_outcome* out, uint32_t n) try {
     if (!j || (n && !out)) return MK_ERR_BAD_ARG;
     for (uint32_t k = 0; k < n; k++) {
         memset(&out[k], 0, sizeof out[k]);
@@ -880,13 +884,22 @@ int mk_job_first_matches(mk_job* j, mk_outcome* out, uint32_t n) {
     for (uint32_t k = 0; k < n; k++) busy += start[k + 1] > start[k];
     const uint32_t threads = std::min<uint32_t>(std::min<uint32_t>(busy, 16u), std::max(1u, std::thread::hardware_concurrency()));
     std::vector<std::thread> pool;
-    for (uint32_t t = 1; t < threads; t++) pool.emplace_back(work);
+    try {
+        pool.reserve(threads);
+        for (uint32_t t = 1; t < threads; t++) pool.emplace_back(work);
+    } catch (...) {
+        // the host would not start another thread (e.g. a process limit): the threads that
+        // did start and this one share the needles
+    }
     work();
     for (auto& t : pool) t.join();
     for (uint32_t k = 0; k < n; k++)
         if (errs[k]) return confirm_fail(j, errs[k]);
+    // candidates beyond the hit ring were counted but not kept: a needle's lowest candidate
+    // may be among them, so the outcomes are those of the kept candidates only
+    if (j->last_total > j->cap) return fail(j->ctx, MK_ERR_HIT_RING_FULL, "hit ring overflow: outcomes of the kept candidates only");
     return MK_OK;
-}
+} MK_ABI_CATCH(j && j->ctx ? &j->ctx->err : nullptr)
 
 int mk_job_io_bytes(const mk_job* j, uint64_t* h2d, uint64_t* d2h) {
     if (!j || !h2d || !d2h) return MK_ERR_BAD_ARG;
@@ -923,16 +936,16 @@ int mk_ctx_work_per_key(const mk_ctx* c, int seed_source, double* field_muls, do
     return MK_OK;
 }
 
-int mk_measure_mad_peaks(mk_ctx* c, double* chain_per_s, double* lo_per_s) {
+int mk_measure_mad_peaks(mk_ctx* c, double* chain_per_s, double* lo_per_s) try {
     if (!c || !chain_per_s || !lo_per_s) return MK_ERR_BAD_ARG;
     MK_CUDA(c, cudaSetDevice(c->device));
     MK_CUDA(c, mkb::measure_mad_peaks((int)c->info.sms, c->stream, chain_per_s, lo_per_s));
     return MK_OK;
-}
+} MK_ABI_CATCH(c ? &c->err : nullptr)
 
 // ---- CUDA graph of a job's launches ----
 
-int mk_job_graph_create(mk_job* j, uint32_t iters, uint32_t launches, mk_graph** out) {
+int mk_job_graph_create(mk_job* j, uint32_t iters, uint32_t launches, mk_graph** out) try {
     if (!j || !out || iters == 0 || launches == 0 || launches > 4096) return MK_ERR_BAD_ARG;
     *out = nullptr;
     mk_ctx* c = j->ctx;
@@ -985,7 +998,7 @@ int mk_job_graph_create(mk_job* j, uint32_t iters, uint32_t launches, mk_graph**
     if (e != cudaSuccess) return bail(e, "cudaGraphInstantiate");
     *out = g;
     return MK_OK;
-}
+} MK_ABI_CATCH(j && j->ctx ? &j->ctx->err : nullptr)
 
 // Points every kernel node at its range of base .. base + launches·span and enqueues the graph.
 static int graph_enqueue(mk_graph* g, uint64_t base) {
@@ -1011,12 +1024,12 @@ static int graph_enqueue(mk_graph* g, uint64_t base) {
     return MK_OK;
 }
 
-int mk_graph_enqueue(mk_graph* g, uint64_t base) {
+int mk_graph_enqueue(mk_graph* g, uint64_t base) try {
     if (!g) return MK_ERR_BAD_ARG;
     return graph_enqueue(g, base);
-}
+} MK_ABI_CATCH(g && g->job && g->job->ctx ? &g->job->ctx->err : nullptr)
 
-int mk_graph_launch(mk_graph* g, uint64_t base, int* found, uint64_t* index) {
+int mk_graph_launch(mk_graph* g, uint64_t base, int* found, uint64_t* index) try {
     if (!g) return MK_ERR_BAD_ARG;
     mk_job* j = g->job;
     j->last.clear();
@@ -1024,9 +1037,9 @@ int mk_graph_launch(mk_graph* g, uint64_t base, int* found, uint64_t* index) {
     if (found) *found = 0;
     if (int st = graph_enqueue(g, base)) return st;
     return collect(j, found, index);
-}
+} MK_ABI_CATCH(g && g->job && g->job->ctx ? &g->job->ctx->err : nullptr)
 
-void mk_graph_destroy(mk_graph* g) {
+void mk_graph_destroy(mk_graph* g) try {
     if (!g) return;
     if (g->job && g->job->ctx) {
         cudaSetDevice(g->job->ctx->device);
@@ -1035,9 +1048,9 @@ void mk_graph_destroy(mk_graph* g) {
     if (g->exec) cudaGraphExecDestroy(g->exec);
     if (g->graph) cudaGraphDestroy(g->graph);
     delete g;
-}
+} MK_ABI_CATCH_VOID
 
-int mk_measure_field_mul(mk_ctx* c, double* radix32_per_s, double* radix26_per_s, double* radix51_fp64_per_s) {
+int mk_measure_field_mul(mk_ctx* c, double* radix32_per_s, double* radix26_per_s, double* radix51_fp64_per_s) try {
     if (!c || !radix32_per_s || !radix26_per_s || !radix51_fp64_per_s) return MK_ERR_BAD_ARG;
     MK_CUDA(c, cudaSetDevice(c->device));
     bool exact = false;
@@ -1045,7 +1058,7 @@ int mk_measure_field_mul(mk_ctx* c, double* radix32_per_s, double* radix26_per_s
                                             radix51_fp64_per_s, &exact));
     if (!exact) return fail(c, MK_ERR_SELF_CHECK, "radix-2^51 (FP64) products differ from radix 2^32");
     return MK_OK;
-}
+} MK_ABI_CATCH(c ? &c->err : nullptr)
 
 int mk_ctx_sync(mk_ctx* c) {
     if (!c) return MK_ERR_BAD_ARG;

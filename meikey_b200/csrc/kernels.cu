@@ -1248,8 +1248,6 @@ cudaError_t measure_field_mul_rates(int sms, cudaStream_t st, double* radix32_pe
 // Derive without allocation: fixed device staging for mk_derive_noalloc
 // ---------------------------------------------------------------------------
 
-#include <mutex>
-
 namespace mkb {
 
 // Device-side staging of the public keys written by mk_derive_noalloc: 65536 keys of 32
@@ -1257,23 +1255,15 @@ namespace mkb {
 // holds it until the process exits, and no call has to allocate device memory for it.
 static __device__ __align__(256) uint8_t g_noalloc_pubkeys[NOALLOC_MAX_KEYS * 32];
 
-// Device address of g_noalloc_pubkeys on `device` (which must be current).  The name of
-// the array in host code is only a host-side stand-in; the address is looked up once per
-// device with cudaGetSymbolAddress and cached.
-cudaError_t noalloc_staging(int device, uint8_t** ptr) {
-    static std::mutex mu;
-    static uint8_t* addr[64];
-    static bool known[64];
-    if (device < 0 || device >= 64) return cudaErrorInvalidDevice;
-    std::lock_guard<std::mutex> lock(mu);
-    if (!known[device]) {
-        void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_pubkeys);
-        if (e != cudaSuccess) return e;
-        addr[device] = static_cast<uint8_t*>(p);
-        known[device] = true;
-    }
-    *ptr = addr[device];
+// Device address of g_noalloc_pubkeys on the current device.  The name of the array in host
+// code is only a host-side stand-in; its address on the device comes from
+// cudaGetSymbolAddress, which the context looks up once when it is created (with its device
+// current) and keeps, so it lives and dies with the context's other device memory.
+cudaError_t noalloc_staging(uint8_t** ptr) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_pubkeys);
+    if (e != cudaSuccess) return e;
+    *ptr = static_cast<uint8_t*>(p);
     return cudaSuccess;
 }
 

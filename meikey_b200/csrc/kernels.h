@@ -65,10 +65,10 @@ cudaError_t keys_occupancy(bool derive, bool incr, uint32_t kpt, uint32_t block,
 // multiply-adds per second of the carry-chain row microbenchmark and of plain mad.lo.u32
 cudaError_t measure_mad_peaks(int sms, cudaStream_t st, double* chain_per_s, double* lo_per_s);
 
-// Largest n of mk_derive_noalloc and the device address of its fixed staging array on
-// `device` (looked up once per device; the device must be current).
+// Largest n of mk_derive_noalloc and the device address of its fixed staging array on the
+// current device (looked up when a context is created).
 constexpr uint64_t NOALLOC_MAX_KEYS = 1ull << 16;
-cudaError_t noalloc_staging(int device, uint8_t** ptr);
+cudaError_t noalloc_staging(uint8_t** ptr);
 cudaError_t launch_build_table(uint4* table, const CombGeom& g, const uint32_t* points, uint64_t first,
                                uint64_t count, cudaStream_t st);
 

@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "../../include/meikey_b200.h"
+#include "abi_guard.h"
 #include "host25519.h"
 
 namespace {
@@ -72,15 +73,15 @@ int emit(const std::string& s, char* out, size_t cap, size_t* written) {
 
 }  // namespace
 
-extern "C" int mk_openssh_public(const uint8_t pk[32], const char* comment, char* out, size_t cap, size_t* written) {
+extern "C" int mk_openssh_public(const uint8_t pk[32], const char* comment, char* out, size_t cap, size_t* written) try {
     if (!pk || !comment || !comment_ok(comment)) return MK_ERR_BAD_ARG;
     std::string line = "ssh-ed25519 " + base64(public_blob(pk));
     if (*comment) line += std::string(" ") + comment;
     return emit(line, out, cap, written);
-}
+} MK_ABI_CATCH(nullptr)
 
 extern "C" int mk_openssh_private(const uint8_t seed[32], const char* comment, uint32_t checkint, char* out,
-                                  size_t cap, size_t* written) {
+                                  size_t cap, size_t* written) try {
     if (!seed || !comment || !comment_ok(comment)) return MK_ERR_BAD_ARG;
     uint8_t pk[32];
     mkh25519::public_key(seed, pk);
@@ -113,4 +114,4 @@ extern "C" int mk_openssh_private(const uint8_t seed[32], const char* comment, u
     wipe(b64);
     wipe(pem);
     return st;
-}
+} MK_ABI_CATCH(nullptr)

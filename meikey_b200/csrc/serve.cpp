@@ -8,10 +8,13 @@
 //   mk_server_*     continuous batching of many jobs (no counterpart in the reference): one
 //                   candidate stream, every tick one launch that tests the needles of all
 //                   admitted jobs; jobs are admitted at tick boundaries as needle slots and
-//                   hit-ring memory free up, shortest expected search first.  A job admitted
+//                   device memory free up, shortest expected search first.  A job admitted
 //                   at stream index a searches [a, a + budget): its result is the lowest
-//                   index there whose key matches (confirmed on the host), which is exactly
-//                   what mk_search of the same job from index a finds alone.
+//                   index there whose key matches (confirmed on the host) and that no other
+//                   job has received, which is what mk_search of the same job from index a
+//                   finds alone once the indices delivered before it are skipped.  One
+//                   index (one secret) goes to one job only, as two runs of the reference
+//                   never share a random key (src/service/gpu.rs:924-925).
 #include <math.h>
 #include <string.h>
 
@@ -20,10 +23,12 @@
 #include <deque>
 #include <memory>
 #include <new>
+#include <set>
 #include <string>
 #include <vector>
 
 #include "../../include/meikey_b200.h"
+#include "abi_guard.h"
 #include "hitsort.h"
 
 namespace {
@@ -74,7 +79,7 @@ int fetch_hits(mk_job* job, std::vector<mk_hit>& hits) {
 
 }  // namespace
 
-extern "C" double mk_expected_tries(const mk_needle* nd) {
+extern "C" double mk_expected_tries(const mk_needle* nd) try {
     if (!nd || !nd->bytes || nd->len == 0) return 0.0;
     if (nd->mode == MK_MODE_REGEX) {
         double p = dfa_match_probability(nd->bytes, nd->len);
@@ -90,13 +95,18 @@ extern "C" double mk_expected_tries(const mk_needle* nd) {
     if (nd->mode == MK_MODE_SUFFIX) rx += '$';
     std::vector<uint8_t> table(4096 * 130);
     uint32_t states = 0;
-    if (mk_regex_compile(rx.c_str(), nd->fold ? 0 : 1, 4096, table.data(), &states, nullptr, 0) != MK_OK) return 0.0;
+    // a needle that no key can match (e.g. a 43-character one whose first character is not
+    // among the 16 values of that position) is refused by the compiler
+    if (mk_regex_compile(rx.c_str(), nd->fold ? 0 : 1, 4096, table.data(), &states, nullptr, 0) != MK_OK)
+        return INFINITY;
     double p = dfa_match_probability(table.data(), states);
     return p > 0 ? 1.0 / p : INFINITY;
+} catch (...) {
+    return 0.0;
 }
 
 extern "C" int mk_search(mk_job* job, const mk_search_config* cfg, mk_progress_fn progress, void* user,
-                         mk_outcome* out) {
+                         mk_outcome* out) try {
     if (!job || !cfg || !out || cfg->iters == 0) return MK_ERR_BAD_ARG;
     memset(out, 0, sizeof *out);
     const double t0 = now_s();
@@ -157,7 +167,7 @@ extern "C" int mk_search(mk_job* job, const mk_search_config* cfg, mk_progress_f
             return MK_OK;
         }
     }
-}
+} MK_ABI_CATCH(nullptr)
 
 // ---------------------------------------------------------------------------
 // continuous batching
@@ -173,6 +183,7 @@ struct ServedJob {
     double expected = 0;     // expected tries
     uint64_t admit = 0;      // stream index at admission
     uint64_t submitted_seq = 0;
+    double device_bytes = 0; // device memory it holds while admitted (estimate at admission)
 };
 
 }  // namespace
@@ -189,6 +200,9 @@ struct mk_server {
     std::vector<mk_job_result> done;
     std::vector<mk_hit> hits;
     bool needles_dirty = true;
+    // stream indices whose key went to a job: each goes to one job only (indices below every
+    // admitted job's start and the stream position can never be hit again and are dropped)
+    std::set<uint64_t> delivered;
 };
 
 static void to_needle(const ServedJob& j, mk_needle& nd) {
@@ -199,7 +213,7 @@ static void to_needle(const ServedJob& j, mk_needle& nd) {
 }
 
 extern "C" int mk_server_create(mk_ctx* ctx, const uint8_t key[32], int seed_source, const mk_server_options* options,
-                                uint64_t first, mk_server** out) {
+                                uint64_t first, mk_server** out) try {
     if (!ctx || !key || !options || !out) return MK_ERR_BAD_ARG;
     const mk_server_options& o = *options;
     if (o.max_jobs == 0 || o.max_jobs > 128 || o.iters_per_tick == 0 || o.budget == 0) return MK_ERR_OUT_OF_RANGE;
@@ -214,15 +228,15 @@ extern "C" int mk_server_create(mk_ctx* ctx, const uint8_t key[32], int seed_sou
     if (st != MK_OK) return st;
     *out = s.release();
     return MK_OK;
-}
+} MK_ABI_CATCH(nullptr)
 
-extern "C" void mk_server_destroy(mk_server* s) {
+extern "C" void mk_server_destroy(mk_server* s) try {
     if (!s) return;
     mk_job_destroy(s->job);
     delete s;
-}
+} MK_ABI_CATCH_VOID
 
-extern "C" int mk_server_submit(mk_server* s, const mk_needle* nd, uint64_t id) {
+extern "C" int mk_server_submit(mk_server* s, const mk_needle* nd, uint64_t id) try {
     if (!s || !nd || !nd->bytes || nd->len == 0) return MK_ERR_BAD_ARG;
     ServedJob j;
     j.id = id;
@@ -237,7 +251,7 @@ extern "C" int mk_server_submit(mk_server* s, const mk_needle* nd, uint64_t id) 
     j.submitted_seq = s->seq++;
     s->queued.push_back(std::move(j));
     return MK_OK;
-}
+} MK_ABI_CATCH(nullptr)
 
 // candidates expected per tick for a job (x sign unknown doubles the rate at worst)
 static double hits_per_tick(const mk_server* s, const ServedJob& j) {
@@ -245,19 +259,36 @@ static double hits_per_tick(const mk_server* s, const ServedJob& j) {
     return j.expected > 0 ? 2.0 * span / j.expected : span;
 }
 
+// hit-ring entries a job reserves: four times its expected candidates per tick, plus 64
+static double ring_entries(const mk_server* s, const ServedJob& j) { return 4.0 * hits_per_tick(s, j) + 64.0; }
+
+// Device memory a job holds while admitted: its reserved hit-ring records (16 bytes each),
+// its DFA table (states x 130 bytes, 16-byte aligned) and its slot of the job state (64 bytes).
+static double job_device_bytes(const mk_server* s, const ServedJob& j) {
+    const double dfa = j.mode == MK_MODE_REGEX ? (double)(((size_t)j.len * 130 + 15) & ~(size_t)15) : 0.0;
+    return 16.0 * ring_entries(s, j) + dfa + 64.0;
+}
+
 static int admit(mk_server* s) {
     if (s->queued.empty()) return MK_OK;
     // shortest expected search first; ties in submission order
     std::stable_sort(s->queued.begin(), s->queued.end(),
                      [](const ServedJob& a, const ServedJob& b) { return a.expected < b.expected; });
-    double ring = 0;
-    for (auto& a : s->active) ring += 4.0 * hits_per_tick(s, a) + 64.0;
+    double ring = 0, mem = 0;
+    for (auto& a : s->active) {
+        ring += ring_entries(s, a);
+        mem += a.device_bytes;
+    }
     std::vector<mk_needle> nds;
     for (auto it = s->queued.begin(); it != s->queued.end();) {
         if (s->active.size() >= s->opt.max_jobs) break;
-        const double need = 4.0 * hits_per_tick(s, *it) + 64.0;
-        if (s->opt.hit_capacity && ring + need > s->opt.hit_capacity && !s->active.empty()) {
-            ++it;  // waits until hit-ring memory frees up (a job is always admitted when none is active)
+        const double need = ring_entries(s, *it), bytes = job_device_bytes(s, *it);
+        // a job waits until hit-ring entries and device memory free up (a job is always
+        // admitted when none is active)
+        const bool ring_full = s->opt.hit_capacity && ring + need > (double)s->opt.hit_capacity;
+        const bool mem_full = s->opt.device_bytes && mem + bytes > (double)s->opt.device_bytes;
+        if ((ring_full || mem_full) && !s->active.empty()) {
+            ++it;
             continue;
         }
         // does it still fit the matcher's shift-and state / regex slots?
@@ -277,7 +308,9 @@ static int admit(mk_server* s) {
         ServedJob j = std::move(*it);
         it = s->queued.erase(it);
         j.admit = s->pos;
+        j.device_bytes = bytes;
         ring += need;
+        mem += bytes;
         s->active.push_back(std::move(j));
         s->needles_dirty = true;
     }
@@ -299,7 +332,7 @@ static void finish(mk_server* s, size_t slot, int status, uint64_t index, uint64
     s->done.push_back(r);
 }
 
-extern "C" int mk_server_tick(mk_server* s, uint32_t* active, uint32_t* queued) {
+extern "C" int mk_server_tick(mk_server* s, uint32_t* active, uint32_t* queued) try {
     if (!s) return MK_ERR_BAD_ARG;
     int st = admit(s);
     if (st) return st;
@@ -345,12 +378,16 @@ extern "C" int mk_server_tick(mk_server* s, uint32_t* active, uint32_t* queued) 
         if (k >= s->active.size() || closed[k]) continue;
         const ServedJob& j = s->active[k];
         if (h.index < j.admit || h.index >= j.admit + s->opt.budget) continue;
+        // hits are in (index, slot) order: of two jobs matching one key, the one admitted
+        // earlier receives it and the other goes on to its next candidate
+        if (s->delivered.count(h.index)) continue;
         int ok = 0;
         st = mk_job_confirm(s->job, h.index, h.needle, pk, secret, &ok);
         if (st != MK_OK) return st;
         if (ok) {
             finish(s, k, MK_OK, h.index, h.index - j.admit + 1, pk, secret);
             closed[k] = 1;
+            s->delivered.insert(h.index);
         }
     }
     s->pos += span;
@@ -369,18 +406,21 @@ extern "C" int mk_server_tick(mk_server* s, uint32_t* active, uint32_t* queued) 
     }
     if (w != s->active.size()) s->needles_dirty = true;
     s->active.resize(w);
+    uint64_t low = s->pos;  // no job will search below this
+    for (const ServedJob& j : s->active) low = std::min(low, j.admit);
+    s->delivered.erase(s->delivered.begin(), s->delivered.lower_bound(low));
     if (active) *active = (uint32_t)s->active.size();
     if (queued) *queued = (uint32_t)s->queued.size();
     return MK_OK;
-}
+} MK_ABI_CATCH(nullptr)
 
-extern "C" int mk_server_results(mk_server* s, mk_job_result* out, uint32_t cap, uint32_t* n) {
+extern "C" int mk_server_results(mk_server* s, mk_job_result* out, uint32_t cap, uint32_t* n) try {
     if (!s || !n || (cap && !out)) return MK_ERR_BAD_ARG;
     const uint32_t k = (uint32_t)std::min<size_t>(cap, s->done.size());
     for (uint32_t i = 0; i < k; i++) out[i] = s->done[i];
     s->done.erase(s->done.begin(), s->done.begin() + k);
     *n = k;
     return MK_OK;
-}
+} MK_ABI_CATCH(nullptr)
 
 extern "C" uint64_t mk_server_position(const mk_server* s) { return s ? s->pos : 0; }

@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "../../include/meikey_b200.h"
+#include "abi_guard.h"
 
 namespace {
 
@@ -129,14 +130,14 @@ static int autotune(int device, mk_tune_entry* entries, uint32_t n, uint32_t fin
 }
 
 extern "C" int mk_autotune(int device, mk_tune_entry* entries, uint32_t n, uint32_t finalists, uint64_t trial_keys,
-                           uint32_t* best) {
+                           uint32_t* best) try {
     const mk_needle nd{(const uint8_t*)TUNE_NEEDLE, (uint32_t)strlen(TUNE_NEEDLE), 0, MK_MODE_CONTAINS};
     return autotune(device, entries, n, finalists, trial_keys, TrialJob{TUNE_KEY, MK_SEED_CHACHA20, &nd, 1}, best);
-}
+} MK_ABI_CATCH(nullptr)
 
 extern "C" int mk_autotune_job(int device, mk_tune_entry* entries, uint32_t n, uint32_t finalists, uint64_t trial_keys,
                                const uint8_t key[32], int seed_source, const mk_needle* needles, uint32_t n_needles,
-                               uint32_t* best) {
+                               uint32_t* best) try {
     if (!key || (n_needles && !needles)) return MK_ERR_BAD_ARG;
     return autotune(device, entries, n, finalists, trial_keys, TrialJob{key, seed_source, needles, n_needles}, best);
-}
+} MK_ABI_CATCH(nullptr)

@@ -388,10 +388,11 @@ class Server:
     """Continuous batching of many jobs over one candidate stream (mk_server_*)."""
 
     def __init__(self, ctx: Context, key: bytes, source: int = L.SEED_CHACHA20, max_jobs: int = 64,
-                 iters_per_tick: int = 8, budget: int = 1 << 26, hit_capacity: int = 0, first: int = 0):
+                 iters_per_tick: int = 8, budget: int = 1 << 26, hit_capacity: int = 0, first: int = 0,
+                 device_bytes: int = 0):
         self.ctx = ctx
         self._lib = ctx._lib
-        opts = L.ServerOptionsC(max_jobs, iters_per_tick, budget, hit_capacity)
+        opts = L.ServerOptionsC(max_jobs, iters_per_tick, budget, hit_capacity, device_bytes)
         ptr = ctypes.c_void_p()
         _check(self._lib, ctx._ptr, self._lib.mk_server_create(ctx._ptr, bytes(key), source, ctypes.byref(opts), first,
                                                                ctypes.byref(ptr)))

@@ -31,7 +31,7 @@ def test_library_exports_every_declared_symbol():
     for name in declared():
         assert hasattr(raw, name), f"{name} declared but not exported"
         assert name in bound, f"{name} not bound in meikey_b200/_lib.py"
-    assert lib.mk_abi_version() == 1
+    assert lib.mk_abi_version() == 2
 
 
 def test_struct_layouts_match_header():

@@ -63,38 +63,96 @@ def _random_needles(n, seed):
     return out
 
 
-def test_server_results_equal_jobs_alone(gpu_ctx, oracle):
-    """24 jobs (two of them practically unmatchable) through 16 slots: each job's result (found key or censoring) is the
-    result of the same needle searched alone from its admission index with a different launch
-    size, and found keys are the oracle's."""
-    key = chacha_key(31)
-    kpi = gpu_ctx.keys_per_iter
-    budget = 24 * kpi + 7
-    needles = _random_needles(22, 5) + [mk.Needle.contains("Zq9xYw7"), mk.Needle.suffix("Qz81a")]
-    results = {}
-    with mk.Server(gpu_ctx, key, max_jobs=16, iters_per_tick=2, budget=budget) as srv:
+def _serve(gpu_ctx, key, needles, budget, **kw):
+    """Runs the jobs through a server; returns their results and the order they finished in."""
+    results, order = {}, []
+    with mk.Server(gpu_ctx, key, budget=budget, **kw) as srv:
         for i, nd in enumerate(needles):
             srv.submit(nd, i)
-        for _ in range(200):
-            active, queued = srv.tick()
+        for _ in range(400):
+            srv.tick()
             for r in srv.results():
                 results[r["id"]] = r
+                order.append(r["id"])
             if len(results) == len(needles):
                 break
     assert len(results) == len(needles)
-    assert any(r["found"] for r in results.values()) and any(not r["found"] for r in results.values())
-    admits = sorted({r["admit_index"] for r in results.values()})
-    assert len(admits) > 1  # some jobs waited for a slot
-    for i, nd in enumerate(needles):
+    return results, order
+
+
+def _alone(gpu_ctx, key, nd, admit, budget, consumed):
+    """The job searched alone from its admission index (a different launch size), skipping the
+    indices already delivered to jobs that finished before it."""
+    first, end = admit, admit + budget
+    with gpu_ctx.job(key, mk.SEED_CHACHA20, [nd]) as job:
+        while True:
+            out = job.search(first=first, max_tries=end - first, iters=3)
+            if not out["found"] or out["index"] not in consumed:
+                return out
+            first = out["index"] + 1
+
+
+def _check_against_alone(gpu_ctx, oracle, key, needles, budget, results, order):
+    consumed = set()
+    for i in order:
         r = results[i]
-        with gpu_ctx.job(key, mk.SEED_CHACHA20, [nd]) as job:
-            alone = job.search(first=r["admit_index"], max_tries=budget, iters=3)
+        alone = _alone(gpu_ctx, key, needles[i], r["admit_index"], budget, consumed)
         assert alone["found"] == r["found"], i
         if r["found"]:
             assert (alone["index"], alone["pk"], alone["secret"]) == (r["index"], r["pk"], r["secret"]), i
             assert r["pk"] == oracle.derive(key, 0, r["index"], 1)
+            consumed.add(r["index"])
         else:
             assert r["tries"] == budget
+
+
+def test_server_results_equal_jobs_alone(gpu_ctx, oracle):
+    """24 jobs (two of them practically unmatchable) through 16 slots: each job's result (found key or censoring) is the
+    result of the same needle searched alone from its admission index with a different launch
+    size (skipping the indices delivered before it), and found keys are the oracle's."""
+    key = chacha_key(31)
+    kpi = gpu_ctx.keys_per_iter
+    budget = 24 * kpi + 7
+    needles = _random_needles(22, 5) + [mk.Needle.contains("Zq9xYw7"), mk.Needle.suffix("Qz81a")]
+    results, order = _serve(gpu_ctx, key, needles, budget, max_jobs=16, iters_per_tick=2)
+    assert any(r["found"] for r in results.values()) and any(not r["found"] for r in results.values())
+    admits = sorted({r["admit_index"] for r in results.values()})
+    assert len(admits) > 1  # some jobs waited for a slot
+    _check_against_alone(gpu_ctx, oracle, key, needles, budget, results, order)
+
+
+def test_server_gives_each_key_to_one_job(gpu_ctx, oracle):
+    """The same needle submitted three times, and needles that match the same keys ('abcd' and
+    'bcd', a folded and an exact copy): every found job gets its own index and secret, the one
+    admitted first the lowest; each result is still the job alone with the indices delivered
+    before it skipped."""
+    key = chacha_key(34)
+    kpi = gpu_ctx.keys_per_iter
+    budget = 64 * kpi
+    needles = [mk.Needle.contains("xY"), mk.Needle.contains("xY"), mk.Needle.contains("xY"),
+               mk.Needle.contains("abc"), mk.Needle.contains("bc"), mk.Needle.contains("Bc", case_sensitive=False),
+               mk.Needle.contains("bc")]
+    results, order = _serve(gpu_ctx, key, needles, budget, max_jobs=8, iters_per_tick=1)
+    found = [r for r in results.values() if r["found"]]
+    assert len(found) == len(needles)
+    assert len({r["index"] for r in found}) == len(found)
+    assert len({r["secret"] for r in found}) == len(found)
+    # the three copies of one needle: admitted together, they take its first three keys in slot order
+    assert results[0]["index"] < results[1]["index"] < results[2]["index"]
+    _check_against_alone(gpu_ctx, oracle, key, needles, budget, results, order)
+
+
+def test_server_admits_by_device_memory(gpu_ctx):
+    """With a device-memory budget for about one job's reservation, the second job waits for the
+    first one's memory (admitted at a later stream index); without it both start together."""
+    key = chacha_key(35)
+    kpi = gpu_ctx.keys_per_iter
+    needles = [mk.Needle.contains("Zq9xY"), mk.Needle.contains("Wv8uT")]
+    # one job holds 16 * (4 * expected candidates per tick + 64) + 64 bytes: about 1.1 KB here
+    res_tight, _ = _serve(gpu_ctx, key, needles, 2 * kpi, max_jobs=8, iters_per_tick=1, device_bytes=1500)
+    res_free, _ = _serve(gpu_ctx, key, needles, 2 * kpi, max_jobs=8, iters_per_tick=1)
+    assert res_free[0]["admit_index"] == res_free[1]["admit_index"]
+    assert res_tight[1]["admit_index"] > res_tight[0]["admit_index"]
 
 
 def test_server_admits_shortest_expected_first(gpu_ctx):

@@ -43,6 +43,25 @@ def test_largest_size_and_reuse(ctx):
     assert b == ctx.derive(key_of(4), mk.SEED_CHACHA20, 5, 3)
 
 
+def test_matches_golden_keys_and_oracle(ctx, golden_pubkeys, oracle):
+    """Against fixtures and the oracle, not only mk_derive: the golden ChaCha20 keys 0..4095
+    (pinned by OpenSSL and the reference build), then counter seeds whose indices run past
+    the top of the 64-bit index space (the seed tail wraps), twice in a row."""
+    cha, cnt = golden_pubkeys
+    assert ctx.derive_noalloc(key_of(1), mk.SEED_CHACHA20, 0, 4096) == cha
+    assert ctx.derive_noalloc(key_of(1), mk.SEED_COUNTER, 0, 1024) == cnt
+    first, n = 2**64 - 100, 200
+    for _ in range(2):
+        got = ctx.derive_noalloc(key_of(5), mk.SEED_COUNTER, first, n)
+        assert got == oracle.derive(key_of(5), mk.SEED_COUNTER, first, n)
+
+
+def test_incremental_source_is_rejected(ctx):
+    with pytest.raises(mk.GpuError) as e:
+        ctx.derive_noalloc(bytes(31) + b"\x40", mk.SEED_INCREMENTAL, 0, 16)
+    assert e.value.status == _lib.ERR_BAD_ARG
+
+
 def test_oversize_is_rejected(ctx):
     with pytest.raises(mk.GpuError) as e:
         ctx.derive_noalloc(key_of(1), mk.SEED_CHACHA20, 0, _lib.NOALLOC_MAX_KEYS + 1)
