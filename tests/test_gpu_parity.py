@@ -4,6 +4,7 @@ Public keys are bit-exact; candidate hits (y only, x sign unknown) are the exact
 sets the reference matcher gives (src/service/gpu/kernel.cu:1804-1875)."""
 import hashlib
 import random
+import re
 
 import pytest
 
@@ -618,3 +619,40 @@ def test_search_ends_at_the_top_of_the_index_space(gpu_ctx, oracle, source):
         hits, total = job.hits(cap=1 << 18)
     want = oracle.search(key, source, base, kpi, b"Ab", 2, False, 0)
     assert [i for i, _ in hits] == want and total == len(want)
+
+
+def _tail(pk: bytes) -> str:
+    """The 43 searched base64 characters of a public key (after the fixed key prefix)."""
+    import base64
+    blob = b"\x00\x00\x00\x0bssh-ed25519\x00\x00\x00\x20" + pk
+    return base64.b64encode(blob).decode()[25:]
+
+
+@pytest.mark.parametrize("pattern", [r"\b9", r"(?i)ab$", r"\B[0-9]\b", r"(?i)x[[:digit:]]{2}\>"])
+def test_regex_dialect_over_golden_keys(gpu_ctx, golden, oracle, pattern):
+    """Regexes with a word boundary and an inline flag (the reference's own test patterns
+    `\\b9`, dfa.rs:258, and `(?i)ab$`, dfa.rs:288, and two more), compiled by the library, over
+    the golden 65,536 keys: the candidate set is exactly the keys whose searched characters
+    match under Python `re` (ASCII mode, the regex crate's semantics here) with the character
+    that depends on the x sign taken either way, as the GPU tests it."""
+    key = bytes.fromhex(golden["chacha_key"])
+    lo, hi = golden["search_range"]
+    py = pattern.replace(r"\>", r"\b(?<=\w)").replace("[[:digit:]]", "[0-9]")
+    pyre = re.compile(py, re.ASCII)
+    pks = oracle.derive(key, mk.SEED_CHACHA20, lo, hi - lo)
+    want = []
+    for i in range(hi - lo):
+        pk = bytearray(pks[32 * i:32 * i + 32])
+        texts = []
+        for sign in (0, 1):
+            pk[31] = (pk[31] & 0x7F) | (sign << 7)
+            texts.append(_tail(bytes(pk)))
+        if any(pyre.search(t) for t in texts):
+            want.append(lo + i)
+    nd = mk.Needle.regex(pattern)
+    with gpu_ctx.job(key, mk.SEED_CHACHA20, [nd]) as job:
+        job.launch(lo, 1)
+        hits, total = job.hits(cap=1 << 18)
+    assert total == len(hits)
+    assert [i for i, _ in hits if lo <= i < hi] == want, pattern
+    assert want  # every pattern has candidates among these keys
