@@ -593,45 +593,49 @@ static void put_fe_words(fe a, u32* out) {
 /*
  * Row i, column k holds k · 2^(w·i) · 8B as (y+x, y-x, 2dxy), each canonical
  * and packed as 8 LE words; the top row is offset by 2^254·B and row 0 holds
- * 2xy in place of 2dxy (comb.rs:353-392, gpu.rs:1459-1480).
+ * 2xy in place of 2dxy (comb.rs:353-392, gpu.rs:1459-1480).  One row into
+ * `out` (cols x 24 words), so that rows can be built on separate threads
+ * (call mko_init first).
  */
-EXPORT void mko_ref_table(u32 w, u32* out) {
+EXPORT void mko_ref_table_row(u32 w, u32 i, u32* out) {
     oracle_init();
     u64 rows = (251 + w - 1) / w, cols = (1ull << (w - 1)) + 1;
     ge rowbase = BASE;
-    for (int i = 0; i < 3; i++) rowbase = ge_double(rowbase);
+    for (u64 c = 0; c < 3 + (u64)w * i; c++) rowbase = ge_double(rowbase);
     fe* zs = (fe*)malloc(sizeof(fe) * cols);
     fe* pre = (fe*)malloc(sizeof(fe) * cols);
     ge* pts = (ge*)malloc(sizeof(ge) * cols);
-    for (u64 i = 0; i < rows; i++) {
-        ge acc = ge_identity();
-        if (i == rows - 1) {
-            ge top = rowbase;
-            for (u64 c = 0; c < 251 - w * (rows - 1); c++) top = ge_double(top);
-            acc = top;
-        }
-        for (u64 k = 0; k < cols; k++) {
-            pts[k] = acc;
-            acc = ge_add(acc, rowbase);
-        }
-        /* batch inversion of the z coordinates */
-        fe run = fe_one();
-        for (u64 k = 0; k < cols; k++) { pre[k] = run; run = fe_mul(run, pts[k].z); }
-        fe inv = fe_invert(run);
-        for (u64 k = cols; k-- > 0;) { zs[k] = fe_mul(inv, pre[k]); inv = fe_mul(inv, pts[k].z); }
-        for (u64 k = 0; k < cols; k++) {
-            fe x = fe_mul(pts[k].x, zs[k]), y = fe_mul(pts[k].y, zs[k]);
-            u32* e = out + (i * cols + k) * 24;
-            put_fe_words(fe_add(y, x), e);
-            put_fe_words(fe_sub(y, x), e + 8);
-            fe xy = fe_mul(x, y);
-            put_fe_words(i == 0 ? fe_add(xy, xy) : fe_mul(xy, D2), e + 16);
-        }
-        for (u64 k = 0; k < w; k++) rowbase = ge_double(rowbase);
+    ge acc = ge_identity();
+    if (i == rows - 1) {
+        ge top = rowbase;
+        for (u64 c = 0; c < 251 - w * (rows - 1); c++) top = ge_double(top);
+        acc = top;
+    }
+    for (u64 k = 0; k < cols; k++) {
+        pts[k] = acc;
+        acc = ge_add(acc, rowbase);
+    }
+    /* batch inversion of the z coordinates */
+    fe run = fe_one();
+    for (u64 k = 0; k < cols; k++) { pre[k] = run; run = fe_mul(run, pts[k].z); }
+    fe inv = fe_invert(run);
+    for (u64 k = cols; k-- > 0;) { zs[k] = fe_mul(inv, pre[k]); inv = fe_mul(inv, pts[k].z); }
+    for (u64 k = 0; k < cols; k++) {
+        fe x = fe_mul(pts[k].x, zs[k]), y = fe_mul(pts[k].y, zs[k]);
+        u32* e = out + k * 24;
+        put_fe_words(fe_add(y, x), e);
+        put_fe_words(fe_sub(y, x), e + 8);
+        fe xy = fe_mul(x, y);
+        put_fe_words(i == 0 ? fe_add(xy, xy) : fe_mul(xy, D2), e + 16);
     }
     free(zs);
     free(pre);
     free(pts);
+}
+
+EXPORT void mko_ref_table(u32 w, u32* out) {
+    u64 rows = (251 + w - 1) / w, cols = (1ull << (w - 1)) + 1;
+    for (u64 i = 0; i < rows; i++) mko_ref_table_row(w, (u32)i, out + i * cols * 24);
 }
 
 /* signed radix-2^w digits of m = bits 3..253 of a clamped scalar (comb.rs:414-445) */

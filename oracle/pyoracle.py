@@ -18,7 +18,7 @@ _lib = None
 def build():
     """Compile liboracle.so (and the reference CPU build when its sources are present)."""
     subprocess.run(["make", "-s", "-C", HERE, "liboracle.so"], check=True)
-    ref_src = os.environ.get("REF", "/root/reference")
+    ref_src = os.environ.get("REF", os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference"))
     if os.path.exists(os.path.join(ref_src, "src/service/gpu/kernel.cu")):
         subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={ref_src}"], check=True)
 

@@ -25,7 +25,7 @@ sys.path.insert(0, HERE)
 from oracle import pyoracle as po  # noqa: E402
 import dfa_builder  # noqa: E402
 
-REF = os.environ.get("REF", "/root/reference")
+REF = os.environ.get("REF", os.path.join(os.path.dirname(ROOT), "reference"))
 
 
 def chacha_key(seed: int) -> bytes:
