@@ -82,6 +82,13 @@ typedef struct mk_options {
     uint32_t inverter_rotates;/* 0: a search CTA's last warp only inverts the CTA's products; 1: every warp
                                  derives keys and the inversion rotates over four warps, one per SM
                                  sub-partition (pays with long iterations: many needles).  Not with hash_warps */
+    uint32_t inversion_batch; /* keys sharing one field inversion (the batch of Montgomery's trick, the
+                                 reference's MEIKEY_BATCH x 4 pooled threads, kernel.cu:2024-2028):
+                                 keys_per_thread x compute threads / pools, for pools a divisor of the
+                                 compute threads (480; 512 with inverter_rotates; 352 with hash_warps) of
+                                 at most 32, e.g. 256 = 8 x 480 / 15.  0: 32 pools (keys_per_thread x 15,
+                                 x 16 with inverter_rotates, x 11 with hash_warps); else
+                                 MK_ERR_OUT_OF_RANGE when no pool count gives it */
 } mk_options;
 
 /* One pattern as the reference's GPU needle (Needle, src/service/gpu.rs:618-660):
@@ -115,6 +122,8 @@ typedef struct mk_info {
     uint64_t table_bytes;
     uint64_t keys_per_iter;   /* grid · (block - 32; block with inverter_rotates; 352 with hash_warps) · keys_per_thread */
     char name[96];
+    uint32_t inversion_batch; /* keys sharing one field inversion */
+    uint32_t reserved;
 } mk_info;
 
 /* One candidate of the autotuner and what it measured. */

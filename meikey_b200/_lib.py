@@ -49,6 +49,7 @@ class Options(ctypes.Structure):
         ("hit_capacity", ctypes.c_uint32),
         ("hash_warps", ctypes.c_uint32),
         ("inverter_rotates", ctypes.c_uint32),
+        ("inversion_batch", ctypes.c_uint32),
     ]
 
 
@@ -106,6 +107,8 @@ class InfoC(ctypes.Structure):
         ("table_bytes", ctypes.c_uint64),
         ("keys_per_iter", ctypes.c_uint64),
         ("name", ctypes.c_char * 96),
+        ("inversion_batch", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32),
     ]
 
 

@@ -40,6 +40,7 @@ struct mk_ctx {
     uint32_t kpt = 8, block = 256, grid = 0;
     uint32_t hash_warps = 0;  // 4: search kernel with hashing warps (ChaCha20 / counter seeds)
     uint32_t layout = mkb::LAYOUT_INVERTER_WARP;  // division of work inside a search CTA
+    uint32_t inv_pools = 32;  // field inversions per search CTA and iteration
     uint32_t hit_capacity = 1u << 16;
     uint8_t* noalloc = nullptr;  // device address of mk_derive_noalloc's fixed staging array
     std::string err;
@@ -243,6 +244,20 @@ int mk_ctx_create(int device, const mk_options* options, mk_ctx** out) try {
     if (o.table_rows < 10 || o.table_rows > (uint32_t)mkb::MAX_ROWS || !built || !hw_ok || !rot_ok ||
         o.blocks_per_sm > 16 || o.hit_capacity > (1u << 26))
         return MK_ERR_OUT_OF_RANGE;
+    // inversion batch: keys per field inversion = keys per thread x compute threads / pools, with
+    // the pools a divisor of the compute threads and at most 32 (one per lane of the inverting warp)
+    const uint32_t layout = o.hash_warps ? mkb::LAYOUT_HASH_WARPS : o.inverter_rotates ? mkb::LAYOUT_ROTATING
+                                                                                       : mkb::LAYOUT_INVERTER_WARP;
+    const uint32_t ct = mkb::search_threads(o.block, layout);
+    uint32_t pools = 32;
+    if (o.inversion_batch) {
+        const uint64_t keys = (uint64_t)ct * o.keys_per_thread;
+        if (keys % o.inversion_batch) return MK_ERR_OUT_OF_RANGE;
+        pools = (uint32_t)(keys / o.inversion_batch);
+        if (pools == 0 || pools > 32 || ct % pools) return MK_ERR_OUT_OF_RANGE;
+    } else if (ct % 32) {
+        return MK_ERR_OUT_OF_RANGE;
+    }
     mk_ctx* c = new (std::nothrow) mk_ctx;
     if (!c) return MK_ERR_OUT_OF_MEMORY;
     *out = c;
@@ -250,7 +265,8 @@ int mk_ctx_create(int device, const mk_options* options, mk_ctx** out) try {
     c->kpt = o.keys_per_thread;
     c->block = o.block;
     c->hash_warps = o.hash_warps;
-    c->layout = o.hash_warps ? mkb::LAYOUT_HASH_WARPS : o.inverter_rotates ? mkb::LAYOUT_ROTATING : mkb::LAYOUT_INVERTER_WARP;
+    c->layout = layout;
+    c->inv_pools = pools;
     if (o.hit_capacity) c->hit_capacity = o.hit_capacity;
     MK_CUDA(c, cudaSetDevice(device));
     MK_CUDA(c, mkb::noalloc_staging(&c->noalloc));
@@ -320,6 +336,7 @@ int mk_ctx_create(int device, const mk_options* options, mk_ctx** out) try {
     // the threads of a search CTA that derive keys (all but a dedicated inverter warp, unless the
     // inversion rotates; 352 comb threads with hashing warps)
     in.keys_per_iter = (uint64_t)c->grid * mkb::search_threads(c->block, c->layout) * c->kpt;
+    in.inversion_batch = mkb::search_threads(c->block, c->layout) * c->kpt / c->inv_pools;
     snprintf(in.name, sizeof in.name, "%.95s", prop.name);
     if (o.self_check) {
         int st = self_check(c);
@@ -707,6 +724,7 @@ static mkb::KeyLaunch search_params(const mk_job* j, uint64_t base, uint32_t ite
     if (j->source == MK_SEED_INCREMENTAL) set_incremental(c, j->key, base, L);
     L.dfa_smem = dfa_smem_bytes(j);
     L.layout = c->layout;
+    L.inv_pools = c->inv_pools;
     return L;
 }
 
@@ -915,7 +933,7 @@ int mk_ctx_work_per_key(const mk_ctx* c, int seed_source, double* field_muls, do
     // a squaring 28 cross products + 8 diagonal ones (72) + 16
     const double MUL = 144.0, SQ = 88.0;
     const double kpt = c->kpt, rows = c->geom.rows;
-    const double ct = mkb::search_threads(c->block, c->layout), groups = ct / 32.0;
+    const double ct = mkb::search_threads(c->block, c->layout);
     // comb: row 0 is free, full additions cost 7 multiplications, the last one 3
     double comb = 7.0 * (rows - 2) + 3.0;
     // Montgomery batch inside a thread: a_j and the running product (2 each for j > 0),
@@ -927,10 +945,11 @@ int mk_ctx_work_per_key(const mk_ctx* c, int seed_source, double* field_muls, do
         // (at most 8 additions per launch) is left out
         comb = (3.0 * (kpt - 1) + 7.0) / kpt;
     }
-    // pooled inversion by the CTA's inverter warp: each lane a pool of `groups` thread
+    // pooled inversion by the CTA's inverting warp: `pools` lanes, each over `groups` thread
     // products, 3(groups-1) multiplications and one inversion (254 squarings + 11 multiplications)
-    double pool_mul = 32.0 * (3.0 * (groups - 1) + 11.0) / (ct * kpt);
-    double pool_sq = 32.0 * 254.0 / (ct * kpt);
+    const double pools = c->inv_pools, groups = ct / pools;
+    double pool_mul = pools * (3.0 * (groups - 1) + 11.0) / (ct * kpt);
+    double pool_sq = pools * 254.0 / (ct * kpt);
     *field_muls = comb + batch + pool_mul + pool_sq;
     *int_mads = (comb + batch + pool_mul) * MUL + pool_sq * SQ;
     return MK_OK;

@@ -433,23 +433,27 @@ __device__ __forceinline__ void backward(const KeyLaunch& L, const MatchSet& ms,
 __device__ __forceinline__ void bar_sync(int id, int count) { asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(count) : "memory"); }
 __device__ __forceinline__ void bar_arrive(int id, int count) { asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(count) : "memory"); }
 
-// Inverts `groups`·32 products in place: lane l of the calling warp handles the strided
-// pool l, l+32, l+64, ... (Montgomery's trick inside each pool).
-__device__ __forceinline__ void invert_pools(fe* prod, fe* scratch, int groups) {
+// Inverts the `pools`·`groups` products prod[0 .. pools·groups) in place with one field
+// inversion per pool: lane l < pools of the calling warp handles the strided pool l, l+pools,
+// l+2·pools, ... (Montgomery's trick inside each pool); the other lanes idle.  With 32 pools
+// every lane works; fewer pools share each inversion among more keys (the inversion batch of a
+// pool is groups x the keys per thread).
+__device__ __forceinline__ void invert_pools(fe* prod, fe* scratch, int groups, int pools = 32) {
     const int l = threadIdx.x & 31;
+    if (l >= pools) return;
     fe acc = prod[l];
     scratch[l] = acc;
 #pragma unroll 1
     for (int k = 1; k < groups; k++) {
-        acc = mk32::fe_mul(acc, prod[l + 32 * k]);
-        scratch[l + 32 * k] = acc;
+        acc = mk32::fe_mul(acc, prod[l + pools * k]);
+        scratch[l + pools * k] = acc;
     }
     fe inv = mk32::fe_invert(acc);
 #pragma unroll 1
     for (int k = groups - 1; k > 0; k--) {
-        fe t = mk32::fe_mul(inv, scratch[l + 32 * (k - 1)]);
-        inv = mk32::fe_mul(inv, prod[l + 32 * k]);
-        prod[l + 32 * k] = t;
+        fe t = mk32::fe_mul(inv, scratch[l + pools * (k - 1)]);
+        inv = mk32::fe_mul(inv, prod[l + pools * k]);
+        prod[l + pools * k] = t;
     }
     prod[l] = inv;
 }
@@ -540,6 +544,9 @@ __device__ __forceinline__ void incr_fracs(const ge& Q, const uint4* steps, Batc
 //     BLOCK/32 - 4 + it % 4, one warp per sub-partition in turn.  The sub-partitions carry
 //     equal shares, but the inverting warp starts its next iteration only after the chain.
 //     That pays when iterations are long (many needles) and costs when they are short.
+// The CTA's CT products of an iteration are inverted in L.inv_pools pools (default 32: lane l
+// of the inverting warp takes threads l, l+32, ...), one field inversion each, so one
+// inversion serves KPT·CT/pools keys.
 // Named barriers, all BLOCK threads: products of buffer b ready (1 + b): the inverting warp
 // waits, the others arrive; inverses of buffer b ready (3 + b): the inverting warp arrives,
 // the others wait.  Stop requests (host stop word, or a hit with stop_on_hit) are read by
@@ -551,7 +558,7 @@ __device__ __forceinline__ void incr_fracs(const ge& Q, const uint4* steps, Batc
 template <int KPT, int BLOCK, bool INCR, bool ROT>
 __global__ void __launch_bounds__(BLOCK, 512 / BLOCK) k_search(const KeyLaunch L) {
     constexpr int CT = ROT ? BLOCK : BLOCK - 32;  // compute threads
-    constexpr int CW = CT / 32;                   // compute warps = pool length per inverting lane
+    constexpr int CW = CT / 32;                   // compute warps
     extern __shared__ uint4 dyn_smem[];
     fe (*prod)[CT] = reinterpret_cast<fe (*)[CT]>(dyn_smem);
     fe (*scratch)[CT] = prod + 2;
@@ -606,6 +613,8 @@ __global__ void __launch_bounds__(BLOCK, 512 / BLOCK) k_search(const KeyLaunch L
     __syncthreads();
     const u32 iters = L.iters;
     if (iters == 0) return;
+    // inversion pools of the CTA (a divisor of CT, at most 32; the host checks it)
+    const int pools = L.inv_pools ? (int)L.inv_pools : 32;
 
     if (!ROT && tid >= (u32)CT) {
         // ---- dedicated inverter warp ----
@@ -620,7 +629,7 @@ __global__ void __launch_bounds__(BLOCK, 512 / BLOCK) k_search(const KeyLaunch L
                 }
             }
             __syncwarp();
-            invert_pools(prod[b], scratch[b], CW);
+            invert_pools(prod[b], scratch[b], CT / pools, pools);
             __syncwarp();
             bar_arrive(3 + b, BLOCK);
             if (it + 1 >= iters || it + 1 >= stop_iter) break;
@@ -661,7 +670,7 @@ __global__ void __launch_bounds__(BLOCK, 512 / BLOCK) k_search(const KeyLaunch L
                 }
             }
             __syncwarp();
-            invert_pools(prod[b], scratch[b], CW);
+            invert_pools(prod[b], scratch[b], CT / pools, pools);
             __syncwarp();
             bar_arrive(3 + b, BLOCK);
         } else {
@@ -738,6 +747,7 @@ __global__ void __launch_bounds__(BLOCK, 1) k_search_hw(const KeyLaunch L) {
     if (iters == 0) return;
     const u64 nthreads = (u64)gridDim.x * CT;
     auto first_of = [&](u32 it, u64 gid) { return L.base + ((u64)it * nthreads + gid) * KPT; };
+    const int pools = L.inv_pools ? (int)L.inv_pools : 32;  // a divisor of CT, at most 32
 
     if (warp > (u32)INV_WARP) {
         // ---- hashing warps ----
@@ -794,7 +804,7 @@ __global__ void __launch_bounds__(BLOCK, 1) k_search_hw(const KeyLaunch L) {
             const bool more = it + 1 < iters && it + 1 < stop_iter;
             // the hashing warps wait on this decision only when they will consider iteration it+2
             if (it + 2 < iters && more) bar_arrive(9 + (it & 1), B_STOP);
-            invert_pools(prod[b], scratch[b], CW);
+            invert_pools(prod[b], scratch[b], CT / pools, pools);
             __syncwarp();
             bar_arrive(3 + b, B_PIPE);
             if (!more) break;

@@ -33,6 +33,10 @@ struct KeyLaunch {
     uint32_t dfa_smem;
     // division of work inside a search CTA (LAYOUT_*)
     uint32_t layout;
+    // field inversions per CTA and iteration (0: 32, one per lane of the inverting warp): each
+    // pools the products of compute threads / inv_pools threads; a divisor of the compute
+    // threads, at most 32
+    uint32_t inv_pools;
 };
 
 // LAYOUT_INVERTER_WARP: the last warp inverts, the others compute keys; LAYOUT_ROTATING: every

@@ -79,10 +79,10 @@ class Context:
 
     def __init__(self, device: int = 0, table_rows: int = 12, keys_per_thread: int = 16, block: int = 512,
                  blocks_per_sm: int = 0, self_check: bool = False, hit_capacity: int = 0, hash_warps: int = 0,
-                 inverter_rotates: bool = False):
+                 inverter_rotates: bool = False, inversion_batch: int = 0):
         self._lib = L.load()
         opts = L.Options(table_rows, keys_per_thread, block, blocks_per_sm, 1 if self_check else 0, hit_capacity,
-                         hash_warps, 1 if inverter_rotates else 0)
+                         hash_warps, 1 if inverter_rotates else 0, inversion_batch)
         ptr = ctypes.c_void_p()
         st = self._lib.mk_ctx_create(device, ctypes.byref(opts), ctypes.byref(ptr))
         self._ptr = ptr
@@ -348,15 +348,40 @@ class Graph:
 BUILT_VARIANTS = [(4, 256), (8, 256), (16, 256), (8, 512), (16, 512)]
 
 
+def compute_threads(block: int, hash_warps: int = 0, inverter_rotates: int = 0) -> int:
+    """Threads of a search CTA that derive keys."""
+    return 352 if hash_warps else block if inverter_rotates else block - 32
+
+
+def inversion_batches(keys_per_thread: int, block: int, hash_warps: int = 0, inverter_rotates: int = 0,
+                      lo: int = 64, hi: int = 512):
+    """The inversion batches in [lo, hi] a layout can run: keys per thread x compute threads /
+    pools, for pool counts that divide the compute threads and are at most 32."""
+    ct = compute_threads(block, hash_warps, inverter_rotates)
+    return sorted({keys_per_thread * ct // p for p in range(1, 33)
+                   if ct % p == 0 and lo <= keys_per_thread * ct // p <= hi})
+
+
 def tune_space(rows=(11, 12, 13, 14, 16), variants=BUILT_VARIANTS, blocks_per_sm=(0,), hash_warps=(0, 4),
-               inverter_rotates=(0,)):
+               inverter_rotates=(0,), inversion_batch=(0,)):
     """Candidate options: comb rows (table size against multiplications per key) x keys per
-    thread and block (inversion batch = keys per thread x compute warps) x CTAs per SM x the
-    hashing-warp layout (built for block 512, keys per thread 8 and 16) x who inverts (a
-    dedicated warp, or a duty rotating over four key warps; not with hashing warps)."""
-    return [dict(table_rows=r, keys_per_thread=k, block=b, blocks_per_sm=s, hash_warps=h, inverter_rotates=v)
-            for r in rows for (k, b) in variants for s in blocks_per_sm for h in hash_warps for v in inverter_rotates
-            if (h == 0 or (b == 512 and k in (8, 16))) and not (h and v)]
+    thread and block x CTAs per SM x the hashing-warp layout (built for block 512, keys per
+    thread 8 and 16) x who inverts (a dedicated warp, or a duty rotating over four key warps;
+    not with hashing warps) x the inversion batch (keys per field inversion; 0 = 32 pools,
+    "all" = every batch of 64..512 the layout can run)."""
+    out = []
+    for r in rows:
+        for (k, b) in variants:
+            for s in blocks_per_sm:
+                for h in hash_warps:
+                    for v in inverter_rotates:
+                        if not (h == 0 or (b == 512 and k in (8, 16))) or (h and v):
+                            continue
+                        batches = inversion_batches(k, b, h, v) if inversion_batch == "all" else inversion_batch
+                        for ib in batches:
+                            out.append(dict(table_rows=r, keys_per_thread=k, block=b, blocks_per_sm=s, hash_warps=h,
+                                            inverter_rotates=v, inversion_batch=ib))
+    return out
 
 
 def autotune(device: int = 0, candidates=None, finalists: int = 3, trial_keys: int = 1 << 27,
@@ -368,7 +393,7 @@ def autotune(device: int = 0, candidates=None, finalists: int = 3, trial_keys: i
     arr = (L.TuneEntryC * len(cands))()
     for i, c in enumerate(cands):
         arr[i].options = L.Options(c["table_rows"], c["keys_per_thread"], c["block"], c.get("blocks_per_sm", 0), 1, 0,
-                                   c.get("hash_warps", 0), c.get("inverter_rotates", 0))
+                                   c.get("hash_warps", 0), c.get("inverter_rotates", 0), c.get("inversion_batch", 0))
     best = ctypes.c_uint32()
     if job is None:
         st = lib.mk_autotune(device, arr, len(cands), finalists, trial_keys, ctypes.byref(best))

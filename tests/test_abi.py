@@ -3,6 +3,8 @@ declares; argument checks and the no-device path return status codes (no GPU nee
 import ctypes
 import os
 import re
+import shutil
+import subprocess
 
 import pytest
 
@@ -34,13 +36,30 @@ def test_library_exports_every_declared_symbol():
     assert lib.mk_abi_version() == 2
 
 
-def test_struct_layouts_match_header():
+STRUCTS = {"Options": "mk_options", "NeedleC": "mk_needle", "HitC": "mk_hit", "InfoC": "mk_info",
+           "TuneEntryC": "mk_tune_entry", "SearchConfigC": "mk_search_config", "OutcomeC": "mk_outcome",
+           "ServerOptionsC": "mk_server_options", "JobResultC": "mk_job_result"}
+
+
+@pytest.mark.skipif(shutil.which("gcc") is None, reason="gcc not installed")
+def test_struct_layouts_match_header(tmp_path):
+    """Every ctypes mirror has the size and field offsets the C compiler gives the header's struct."""
     from meikey_b200 import _lib
-    assert ctypes.sizeof(_lib.Options) == 32
-    assert ctypes.sizeof(_lib.NeedleC) == 24
-    assert ctypes.sizeof(_lib.HitC) == 16
-    assert ctypes.sizeof(_lib.InfoC) == 4 * 6 + 16 + 96
-    assert ctypes.sizeof(_lib.TuneEntryC) == 32 + 4 + 4 + 8
+    src = ['#include <stddef.h>', '#include <stdio.h>', '#include "meikey_b200.h"', 'int main(void) {']
+    for py, c in STRUCTS.items():
+        src.append(f'    printf("{py} size %zu\\n", sizeof({c}));')
+        for f, _ in getattr(_lib, py)._fields_:
+            src.append(f'    printf("{py} {f} %zu\\n", offsetof({c}, {f}));')
+    src.append("    return 0;\n}")
+    (tmp_path / "layout.c").write_text("\n".join(src))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c99", "-I", os.path.join(ROOT, "include"), str(tmp_path / "layout.c"), "-o", str(exe)],
+                   check=True)
+    for line in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.splitlines():
+        py, field, value = line.split()
+        cls = getattr(_lib, py)
+        got = ctypes.sizeof(cls) if field == "size" else getattr(cls, field).offset
+        assert got == int(value), (py, field)
 
 
 def test_bad_arguments_return_status():
