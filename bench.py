@@ -1,22 +1,30 @@
 """Benchmark of the candidate-key search path (one JSON line on rank 0).
 
-Default workload (the reference's throughput configuration, synthetic inputs): secure-path
-seeds from ChaCha20 with key SHA-256(u64 7 little-endian), a case-sensitive 7-character
-contains needle drawn uniformly from the base64 alphabet with numpy.random.default_rng(7),
-2^34 candidates in total.  A step is one launch over >= 2^30 consecutive candidate indices;
-the default 16 steps cover 2^34.
+Headline (the reference's throughput configuration, synthetic inputs): secure-path seeds
+from ChaCha20 with key SHA-256(u64 7 little-endian), a case-sensitive 7-character contains
+needle drawn uniformly from the base64 alphabet with numpy.random.default_rng(7), inversion
+batched over 256 keys, 2^34 candidates in total.  A step is one launch over >= 2^30
+consecutive candidate indices; the default 16 steps cover 2^34.
 
---workload incremental: the low-security incremental path.  The start scalar is
-clamp(SHA-512(ChaCha20 seed 0 of key SHA-256(u64 11))), index k is the point (s0 + k)·B,
-the needle is a case-sensitive 6-character suffix drawn with numpy.random.default_rng(11),
-2^32 candidates (16 steps of >= 2^28).
+On one GPU the same line carries `workloads`, one record each (value, clocks, roofline, e2e)
+for the other configurations:
+  counter      the reference's published GPU mode: low-security counter seeds, needle TARGET
+               case-insensitive (8 steps of 2^30);
+  incremental  P_k = P_0 + k·B from s0 = clamp(SHA-512(ChaCha20 seed 0 of key SHA-256(u64
+               11))), a case-sensitive 6-character suffix (numpy.random.default_rng(11)),
+               2^32 candidates (16 steps of 2^28);
+  multi        64 text patterns and 8 regexes in one job, each step a CUDA-graph replay of 4
+               launches, 2^34 candidates;
+  serving      1000 Poisson-arriving jobs through continuous batching against one job at a
+               time (p50/p99 time to key).
+--workload <name> measures one of them as the headline; --headline-only skips the others.
 
 Multi-GPU: one process per GPU (torchrun), each rank searches its own index range
 (rank·2^56 ...), so the work is weakly scaled with no data-path collective; timing is the
 max over ranks.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload secure|incremental]
+                    [--workload secure|counter|incremental|multi|serving] [--headline-only]
 """
 import argparse
 import hashlib
@@ -37,12 +45,17 @@ UNIT = "keys/s"
 ALPHABET = "ABCDEFGHIJKLMNOPQRSTUVWXYZabcdefghijklmnopqrstuvwxyz0123456789+/"
 # per workload: total candidates, candidates per step, seed source, generator seed, needle length, mode
 WORKLOADS = {
-    "secure": {"total": 1 << 34, "step": 1 << 30, "source": 0, "seed": 7, "length": 7, "mode": "contains"},
+    "secure": {"total": 1 << 34, "step": 1 << 30, "source": 0, "seed": 7, "length": 7, "mode": "contains",
+               "inversion_batch": 256},
+    # the reference's published GPU mode (docs/benchmark.md): low-security counter seeds, the
+    # needle TARGET case-insensitive
+    "counter": {"total": 1 << 33, "step": 1 << 30, "source": 1, "seed": 7, "length": 0, "mode": "contains_ci",
+                "needle": "TARGET", "inversion_batch": 256},
     "incremental": {"total": 1 << 32, "step": 1 << 28, "source": 2, "seed": 11, "length": 6, "mode": "suffix"},
     "multi": {"total": 1 << 34, "step": 1 << 30, "source": 0, "seed": 23, "length": 0, "mode": "mixed",
               "launches": 4, "inverter_rotates": True},
     "serving": {"total": 0, "step": 0, "source": 0, "seed": 31, "length": 0, "mode": "mixed", "jobs": 1000,
-                "rate": 50.0, "budget": 1 << 26, "iters_per_tick": 8},
+                "rate": 50.0, "budget": 1 << 26, "iters_per_tick": 8, "device_bytes": 32 << 20},
 }
 
 
@@ -122,6 +135,8 @@ MULTI_SET = "all"
 def workload_needle(name: str = "secure") -> str:
     import numpy as np
     w = WORKLOADS[name]
+    if "needle" in w:
+        return w["needle"]
     if name == "multi":
         text = [] if MULTI_SET == "regex" else [t for t, _ in multi_patterns()]
         rx = [] if MULTI_SET == "text" else list(MULTI_REGEXES)
@@ -140,8 +155,10 @@ def workload_needles(name: str = "secure"):
             else:
                 out.append(mk.Needle.contains(text, case_sensitive=mode == "contains"))
         return out + ([mk.Needle.regex(r, max_states=64) for r in MULTI_REGEXES] if MULTI_SET != "text" else [])
-    n = workload_needle(name)
-    return [mk.Needle.suffix(n) if WORKLOADS[name]["mode"] == "suffix" else mk.Needle.contains(n)]
+    n, mode = workload_needle(name), WORKLOADS[name]["mode"]
+    if mode == "suffix":
+        return [mk.Needle.suffix(n)]
+    return [mk.Needle.contains(n, case_sensitive=mode != "contains_ci")]
 
 
 class ClockSampler:
@@ -260,8 +277,9 @@ class CpuBaseline:
         self.threads = os.cpu_count() or 1
         self.source = WORKLOADS[workload]["source"]
         self.mode = 1 if WORKLOADS[workload]["mode"] == "suffix" else 0
+        self.fold = WORKLOADS[workload]["mode"] == "contains_ci"
         variants = [p for p in pyoracle.ref_variants() if "f8_b32" in p] or pyoracle.ref_variants()
-        if variants and self.source == 0:
+        if variants and self.source in (0, 1):
             self.kind = "reference"
             self.ref = pyoracle.RefKernel(variants[0])
             self.width = 16
@@ -276,12 +294,12 @@ class CpuBaseline:
     def run(self, key: bytes, needle: str, seconds: float, base: int = 0):
         """keys/s over a sample of about `seconds` of work on all threads."""
         from concurrent.futures import ThreadPoolExecutor
-        nb = needle.encode()
+        nb = needle.lower().encode() if self.fold else needle.encode()
         if self.ref is not None:
             per_call = 128 * self.ref.batch  # one block of the emulated kernel per iteration
 
             def job(t, iters):
-                self.ref.search(128, self.table, self.width, key, False, nb, len(nb), False, 0,
+                self.ref.search(128, self.table, self.width, key, self.source == 1, nb, len(nb), self.fold, self.mode,
                                 base + t * (1 << 40), iters, False)
             # calibrate
             t0 = time.perf_counter()
@@ -295,7 +313,7 @@ class CpuBaseline:
             keys = self.threads * per_call * iters
         else:
             def job(t, n):
-                self.po.search(key, self.source, base + t * (1 << 40), n, nb, len(nb), False, self.mode, threads=1)
+                self.po.search(key, self.source, base + t * (1 << 40), n, nb, len(nb), self.fold, self.mode, threads=1)
             t0 = time.perf_counter()
             job(0, 2000)
             per_key = max((time.perf_counter() - t0) / 2000, 1e-7)
@@ -344,6 +362,14 @@ def run_reference(args):
                                       if args.workload in ("multi", "serving") else "")},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    if args.workload == "secure" and not args.headline_only:
+        # the reference's published mode (counter seeds, TARGET case-insensitive) on the same cores
+        ccpu = CpuBaseline("counter")
+        rate, ckeys = ccpu.run(workload_key("counter"), workload_needle("counter"), 4 * per_step)
+        line["workloads"] = {"counter": {
+            "value": rate, "unit": UNIT, "config": workload_config("counter", None),
+            "cpu_baseline": {"value": rate, "unit": UNIT, "cores": ccpu.threads, "kind": ccpu.kind,
+                             "sample": f"{ckeys} candidates; {ccpu.what}"}}}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -357,6 +383,14 @@ def workload_config(workload, ctx, step_candidates=None, steps=None):
                         "one CUDA-graph replay of 4 persistent launches; 2^34 candidates",
             "candidates_total": WORKLOADS[workload]["total"],
             "regexes": MULTI_REGEXES,
+        }
+    elif workload == "counter":
+        cfg = {
+            "workload": "the reference's published GPU mode: low-security counter seeds (key SHA-256(u64 7) with "
+                        "the index added to its last 8 bytes), SHA-512 with the per-launch midstate, clamp, comb "
+                        "multiply, pooled inversion, base64, needle 'TARGET' case-insensitive contains; 2^33 "
+                        "candidates",
+            "candidates_total": WORKLOADS[workload]["total"],
         }
     elif workload == "incremental":
         cfg = {
@@ -383,8 +417,8 @@ def workload_config(workload, ctx, step_candidates=None, steps=None):
             "keys_per_thread": info["keys_per_thread"],
             "block": info["block"],
             "grid": info["grid"],
-            # keys sharing one field inversion: a thread's batch times the compute warps pooled per lane
-            "inversion_batch": info["keys_per_iter"] // (info["grid"] * 32),
+            # keys sharing one field inversion (mk_options.inversion_batch)
+            "inversion_batch": info["inversion_batch"],
             "l2": ("no memory-resident inputs: each thread steps its own point, the 14 KB step tables "
                    "stay on chip" if workload == "incremental" else
                    "inputs larger than L2: random gathers from the comb table in HBM"),
@@ -412,7 +446,13 @@ def _pct(xs, q):
 
 
 def run_serving(args):
-    """Continuous batching against one job at a time on the same GPU, same jobs, same keys."""
+    print(json.dumps(serving(args)), flush=True)
+    return 0
+
+
+def serving(args):
+    """Continuous batching against one job at a time on the same GPU, same jobs, same keys:
+    the JSON record of the serving workload."""
     import meikey_b200 as mk
     wl = WORKLOADS["serving"]
     n_jobs = args.serve_jobs or wl["jobs"]
@@ -423,8 +463,8 @@ def run_serving(args):
     needles = [needle(t, m) for _, t, m in jobs]
     key = hashlib.sha256(wl["seed"].to_bytes(8, "little")).digest()
     ctx = mk.Context(device=0, table_rows=args.rows, keys_per_thread=args.kpt or 8, block=args.block, self_check=True,
-                     hit_capacity=1 << 22, inverter_rotates=args.inverter_rotates)
-    budget, iters = wl["budget"], wl["iters_per_tick"]
+                     hit_capacity=1 << 22, inverter_rotates=bool(args.inverter_rotates))
+    budget, iters, device_bytes = wl["budget"], wl["iters_per_tick"], wl["device_bytes"]
     # warm-up: a few ticks of a throw-away server
     with mk.Server(ctx, key, max_jobs=4, iters_per_tick=iters, budget=budget, first=1 << 60) as warm:
         for k in range(3):
@@ -434,9 +474,10 @@ def run_serving(args):
     clocks = ClockSampler(0)
     clocks.start()
     # serving: arrivals in real time, one tick after another while anything is admitted or queued
-    res, done_at = {}, {}
+    res, done_at, order = {}, {}, []
     ticks = 0
-    with mk.Server(ctx, key, max_jobs=128, iters_per_tick=iters, budget=budget, hit_capacity=1 << 21) as srv:
+    with mk.Server(ctx, key, max_jobs=128, iters_per_tick=iters, budget=budget, hit_capacity=1 << 21,
+                   device_bytes=device_bytes) as srv:
         t0 = time.perf_counter()
         i = 0
         busy = False
@@ -460,12 +501,16 @@ def run_serving(args):
             for r in srv.results():
                 res[r["id"]] = r
                 done_at[r["id"]] = t_done
+                order.append(r["id"])
             busy = active + queued > 0
         serve_span = time.perf_counter() - t0
         stream = srv.position
     clk = clocks.stop()
     # one job at a time: FIFO in arrival order, each job searched alone from its admission
-    # index with the same budget (so the keys must be the same)
+    # index with the same budget, skipping the indices the server delivered to jobs that
+    # finished before it (one key goes to one job), so the keys must be the same
+    rank_of = {j: r for r, j in enumerate(order)}
+    delivered = sorted((rank_of[j], res[j]["index"]) for j in res if res[j]["found"])
     base_res, base_done = {}, {}
     limit = min(n_jobs, args.serve_baseline_jobs or n_jobs)
     single = ctx.job(key, mk.SEED_CHACHA20, [needles[0]])  # one job, its needle replaced per request
@@ -476,7 +521,15 @@ def run_serving(args):
         if now < arrival:
             time.sleep(arrival - now)
         single.update([needles[k]])
-        base_res[k] = single.search(first=res[k]["admit_index"], max_tries=budget, iters=iters)
+        taken = {idx for r, idx in delivered if r < rank_of[k]}
+        first, end = res[k]["admit_index"], res[k]["admit_index"] + budget
+        while True:
+            out = single.search(first=first, max_tries=end - first, iters=iters)
+            if not out["found"] or out["index"] not in taken:
+                break
+            first = out["index"] + 1
+        out["tries"] = (out["index"] + 1 if out["found"] else end) - res[k]["admit_index"]
+        base_res[k] = out
         base_done[k] = time.perf_counter() - t0
     base_span = time.perf_counter() - t0
     single.close()
@@ -500,8 +553,9 @@ def run_serving(args):
             "workload": f"serving: {n_jobs} vanity jobs, Poisson arrivals at {wl['rate']:g}/s (numpy default_rng(31)), "
                         "pattern length U{4..8}, mode uniform over case-sensitive contains / suffix / case-insensitive "
                         "contains; continuous batching over one ChaCha20 candidate stream (key SHA-256(u64 31)), "
-                        f"per-job budget {budget} candidates, admission shortest-expected-first by needle slots "
-                        "and hit-ring plan",
+                        f"per-job budget {budget} candidates, admission shortest-expected-first by needle slots, "
+                        f"hit-ring plan and a device-memory budget of {device_bytes} bytes; each found index goes to "
+                        "one job",
             "value_is": "aggregate job-keys/s: candidates searched for each job, summed over jobs, per second of the "
                         "serving run (one candidate tested for n admitted jobs counts n times)",
             "iters_per_tick": iters, "max_jobs": 128, "budget": budget,
@@ -525,23 +579,31 @@ def run_serving(args):
         "speedup_keys_per_s": value / b_value if b_value else None,
         "speedup_jobs_per_s": (n_jobs / serve_span) / (limit / base_span),
         "e2e": {"value": value, "unit": "keys/s", "note": "host wall clock around submit/tick/results, the public API"},
+        "distinct_keys": len({res[k]["index"] for k in res if res[k]["found"]}) == len(ttk),
     }
-    print(json.dumps(line), flush=True)
-    return 0
+    return line
 
 
-def run_ours(args):
-    world, rank, local = dist_env()
-    dist = Dist(world, local)
+def measure(args, workload, steps, e2e_steps, dist, world, rank, local, cpu_seconds=0.0):
+    """One workload on this rank: `steps` device-timed steps (barrier and synchronize on both
+    sides, max over ranks), then `e2e_steps` end-to-end steps through the public API; on rank 0
+    the JSON record of the workload (None on the other ranks)."""
     import meikey_b200 as mk
-    wl = WORKLOADS[args.workload]
-    key, needle, source = workload_key(args.workload), workload_needle(args.workload), wl["source"]
+    wl = WORKLOADS[workload]
+    key, source = workload_key(workload), wl["source"]
     # the multi-pattern workload's 3-character patterns alone give ~1e-3 candidates per key
     kpt = args.kpt or (16 if source == 2 else 8)
+    rotates = args.inverter_rotates if args.inverter_rotates is not None else bool(wl.get("inverter_rotates", False))
+    hash_warps = args.hash_warps if source != 2 else 0
+    inv_batch = args.inversion_batch
+    if inv_batch is None:
+        # the workload's batch where this layout can run it (256 = 8 keys x 480 threads / 15 pools)
+        inv_batch = wl.get("inversion_batch", 0)
+        if inv_batch not in mk.engine.inversion_batches(kpt, args.block, hash_warps, int(rotates), 1, 1 << 20):
+            inv_batch = 0
     ctx = mk.Context(device=local, table_rows=args.rows, keys_per_thread=kpt, block=args.block,
-                     self_check=True, hit_capacity=(1 << 22) if args.workload == "multi" else 0,
-                     hash_warps=args.hash_warps if source != 2 else 0,
-                     inverter_rotates=args.inverter_rotates)
+                     self_check=True, hit_capacity=(1 << 22) if workload == "multi" else 0,
+                     hash_warps=hash_warps, inverter_rotates=rotates, inversion_batch=inv_batch)
     kpi = ctx.keys_per_iter
     launches = wl.get("launches", 1)  # > 1: a step is one replay of a CUDA graph of that many launches
     iters = math.ceil((args.step_candidates or wl["step"]) / (kpi * launches))
@@ -549,7 +611,7 @@ def run_ours(args):
     rank_base = rank_first(rank, 0, step_keys)
     peak, peak_lo = ctx.measure_mad_peaks()
     field_muls, mads_per_key = ctx.work_per_key(source)
-    needles = workload_needles(args.workload)
+    needles = workload_needles(workload)
     job = ctx.job(key, source, needles)
     graph = job.graph(iters, launches) if launches > 1 else None
 
@@ -569,7 +631,7 @@ def run_ours(args):
     ctx.sync()
     ctx.record(0)
     first = rank_first(rank, args.warmup, step_keys)
-    for s in range(args.steps):
+    for s in range(steps):
         enqueue_step(first + s * step_keys)
     ctx.record(1)
     ctx.sync()
@@ -577,12 +639,11 @@ def run_ours(args):
     ms_local = ctx.elapsed_ms(0, 1)
     clk = clocks.stop()
     ms = dist.max(ms_local)
-    keys_all = step_keys * args.steps * world
+    keys_all = step_keys * steps * world
     value = keys_all / (ms / 1000.0)
-    per_gpu = step_keys * args.steps / (ms_local / 1000.0)
+    per_gpu = step_keys * steps / (ms_local / 1000.0)
     # end to end through the public API: prepare (H2D of key + compiled needle), launch,
-    # read the job state and hits back (D2H), confirm every hit on the host
-    e2e_steps = args.e2e_steps or args.steps
+    # read the job state and hits back (D2H), confirm every needle's first key on the host
     h2d = d2h = 0
     found = confirmed = 0
     phases = {"prepare": 0.0, "launch_and_wait": 0.0, "read_hits": 0.0, "confirm": 0.0, "release": 0.0}
@@ -592,10 +653,10 @@ def run_ours(args):
     t0 = time.perf_counter()
     for s in range(e2e_steps):
         tp = time.perf_counter()
-        j = ctx.job(key, source, workload_needles(args.workload))
+        j = ctx.job(key, source, workload_needles(workload))
         g = j.graph(iters, launches) if launches > 1 else None
         tl = time.perf_counter()
-        e2e_base = first + (args.steps + s) * step_keys
+        e2e_base = first + (steps + s) * step_keys
         if g is not None:
             g.launch(e2e_base)
         else:
@@ -623,11 +684,10 @@ def run_ours(args):
     if graph is not None:
         graph.close()
     job.close()
-    ctx_info = dict(ctx.info)
     line = None
     if rank == 0:
         achieved = mads_per_key * per_gpu / 1e12
-        tpk = traffic_per_key(args.workload)
+        tpk = traffic_per_key(workload)
         roofline = {
             "bound": "int_mad", "achieved": achieved, "peak": peak / 1e12, "unit": "Tmad/s",
             "frac": achieved / (peak / 1e12) if peak else None,
@@ -637,39 +697,59 @@ def run_ours(args):
             "peak_mad_lo": peak_lo / 1e12,
             "frac_of_mad_lo": achieved / (peak_lo / 1e12) if peak_lo else None,
             "work_per_key": {"field_muls": field_muls, "int_mads": mads_per_key},
-            "kernel_ms_per_launch": ms_local / args.steps,
+            "kernel_ms_per_launch": ms_local / (steps * launches),
         }
-        cfg = workload_config(args.workload, ctx, step_keys, args.steps)
+        cfg = workload_config(workload, ctx, step_keys, steps)
         cfg["launches_per_step"] = launches
         cfg["options_from"] = "mk_autotune sweeps of rows x keys/thread x block (profiles/autotune_sweep.md)"
-        cfg["hash_warps"] = args.hash_warps if source != 2 else 0
-        cfg["inverter_rotates"] = int(args.inverter_rotates)
+        cfg["hash_warps"] = hash_warps
+        cfg["inverter_rotates"] = int(rotates)
         cfg["needles"] = len(needles)
-        if args.workload == "multi" and MULTI_SET != "all":
+        if workload == "multi" and MULTI_SET != "all":
             cfg["needle_set"] = MULTI_SET + " patterns only"
         line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": steps,
+            "warmup": args.warmup, "ms_per_step": ms / steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u32", "data": "synthetic", "config": cfg, "clocks": clk,
-            "gpu_launches": args.steps * launches,
-            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d // e2e_steps,
-                    "d2h_bytes_per_step": d2h // e2e_steps, "steps": e2e_steps, "candidates": found,
+            "gpu_launches": steps * launches,
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d // max(1, e2e_steps),
+                    "d2h_bytes_per_step": d2h // max(1, e2e_steps), "steps": e2e_steps, "candidates": found,
                     "needles_confirmed_on_host": confirmed,
-                    "ms_per_step_by_phase": {k: round(1000 * v / e2e_steps, 3) for k, v in phases.items()},
+                    "ms_per_step_by_phase": {k: round(1000 * v / max(1, e2e_steps), 3) for k, v in phases.items()},
                     "clocks": e2e_clk},
             "roofline": roofline,
-            "device": ctx_info["name"],
+            "device": ctx.info["name"],
         }
     ctx.close()
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = CpuBaseline(args.workload)
-        what = "the same workload"
-        if args.workload == "multi":  # the reference searches one pattern at a time
-            key, needle = workload_key("secure"), workload_needle("secure")
-            what = f"the secure workload's needle '{needle}' (the reference searches one pattern at a time)"
-        rate, keys = cpu.run(key, needle, args.cpu_seconds)
+    if rank == 0 and world == 1 and cpu_seconds > 0:
+        cpu = CpuBaseline(workload)
+        cpu_key, cpu_needle, what = key, workload_needle(workload), "the same workload"
+        if workload == "multi":  # the reference searches one pattern at a time
+            cpu_key, cpu_needle = workload_key("secure"), workload_needle("secure")
+            what = f"the secure workload's needle '{cpu_needle}' (the reference searches one pattern at a time)"
+        rate, keys = cpu.run(cpu_key, cpu_needle, cpu_seconds)
         line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": cpu.threads, "kind": cpu.kind,
                                 "sample": f"{keys} candidates of {what}; {cpu.what}"}
+    return line
+
+
+# the default run measures the headline workload and, on one GPU, these beside it (steps,
+# end-to-end steps): every configuration the benchmark is quoted on, in one line
+SUB_WORKLOADS = {"counter": (8, 2), "incremental": (16, 4), "multi": (16, 2)}
+
+
+def run_ours(args):
+    world, rank, local = dist_env()
+    dist = Dist(world, local)
+    line = measure(args, args.workload, args.steps, args.e2e_steps or args.steps, dist, world, rank, local,
+                   0.0 if args.no_cpu_baseline else args.cpu_seconds)
+    if world == 1 and args.workload == "secure" and not args.headline_only:
+        # the sub-records of the other configurations (one GPU only: the scaling runs time the
+        # headline alone)
+        line["workloads"] = {}
+        for name, (steps, e2e_steps) in SUB_WORKLOADS.items():
+            line["workloads"][name] = measure(args, name, steps, e2e_steps, dist, world, rank, local)
+        line["workloads"]["serving"] = serving(args)
     if rank == 0:
         print(json.dumps(line), flush=True)
     dist.close()
@@ -705,13 +785,17 @@ def main():
                     help="every warp derives keys and the inversion rotates over four warps "
                          "(mk_options.inverter_rotates; default: on for the multi-pattern workload, "
                          "the layout mk_autotune_job picks for it, off otherwise)")
+    ap.add_argument("--inversion-batch", type=int, default=None,
+                    help="keys per field inversion (mk_options.inversion_batch; default: the workload's, 256 for the "
+                         "secure and counter workloads where the layout can run it, else 32 pools)")
+    ap.add_argument("--headline-only", action="store_true",
+                    help="measure the --workload alone (by default the secure headline also carries the counter, "
+                         "incremental, multi-pattern and serving workloads on one GPU)")
     ap.add_argument("--multi-set", choices=["all", "text", "regex"], default="all",
                     help="multi-pattern workload: search all its patterns, or only the text or regex ones")
     args = ap.parse_args()
     global MULTI_SET
     MULTI_SET = args.multi_set
-    if args.inverter_rotates is None:
-        args.inverter_rotates = bool(WORKLOADS[args.workload].get("inverter_rotates", False))
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "serving":
