@@ -112,9 +112,14 @@ def main():
         got = r.derive(table, width, key1, False, hi_first)[:32 * 16]
         assert got == po.derive(key1, 0, hi_first, 16)
         hi[os.path.basename(r.path)] = got.hex()
-    # checksum over the first 2^20 keys (the small secure-path workload), from the oracle
+    # the small secure-path workload: all 2^20 keys from the reference build itself, equal to
+    # the oracle's key for key; the GPU tests compare against the checksum of all of them
+    from concurrent.futures import ThreadPoolExecutor
     n_full = 1 << 20
+    with ThreadPoolExecutor(os.cpu_count() or 1) as ex:  # ctypes releases the GIL
+        full_ref = b"".join(ex.map(lambda f: ref.derive(table, width, key1, False, f), range(0, n_full, ref.batch)))
     full = po.derive(key1, 0, 0, n_full)
+    assert full_ref == full
     digest = hashlib.sha256(full).hexdigest()
     assert full[:32 * n_cha] == pk_ref
 
@@ -164,6 +169,7 @@ def main():
         "chacha_key_seed": 1,
         "chacha_key": key1.hex(),
         "sha256_of_pubkeys_0_2pow20": digest,
+        "pubkeys_0_2pow20_from": os.path.basename(ref.path) + " (every key equal to the oracle's)",
         "pubkeys_high_first": hi_first,
         "pubkeys_high_by_reference_variant": hi,
         "search_range": [0, n_search],
