@@ -275,6 +275,32 @@ MK_API double mk_expected_tries(const mk_needle* needle);
 MK_API int mk_search(mk_job* job, const mk_search_config* cfg, mk_progress_fn progress, void* user,
                      mk_outcome* out);
 
+/* Searcher::run over several jobs at once (the reference's All, src/service/search.rs:107-180,
+ * one searcher per device): one host thread per job runs mk_search's loop over cfgs[k] (each
+ * job on a context of its own, on one device or several; MK_ERR_BAD_ARG when two jobs share a
+ * context).  The first host-verified key sets every other job's stop word (mk_job_stop), so
+ * their running launches end within two iterations and no new launch starts.  `progress` runs
+ * on the calling thread about every 100 ms with the tries summed over the jobs, and a nonzero
+ * return cancels all; cfgs[0].time_limit_s limits the whole call.  *out is the winner's
+ * outcome with tries summed over every job (Stats of All: completed launches and the winner's
+ * range up to its key) and *winner its position, or status MK_ERR_STOPPED and *winner = n when
+ * no job found a key.  The stop requests are withdrawn before the call returns. */
+MK_API int mk_search_many(mk_job* const* jobs, uint32_t n, const mk_search_config* cfgs, mk_progress_fn progress,
+                          void* user, mk_outcome* out, uint32_t* winner);
+
+/* The GPU and the host cores searching together (the reference's Both, src/service/search.rs:
+ * 86-103): mk_search's loop of `job` over cfg on one host thread, and cpu_threads host threads
+ * that derive keys of the same key stream from index cpu_first upward (chunks of 64
+ * consecutive indices, the host derivation and a full match against every needle of the job),
+ * the reference's CPU Parallel worker in scalar form.  Pick cpu_first away from the GPU's
+ * range.  The first key found by either side stops the other (the job's stop word on the GPU
+ * side); *winner is 0 for the GPU, 1 for the host cores, 2 when none (status MK_ERR_STOPPED,
+ * after cfg->max_tries on the GPU side together with the time limit or a cancel from
+ * `progress`, which runs on the calling thread about every 100 ms; the host cores search
+ * until a key, the time limit or a cancel).  Tries are summed over both sides. */
+MK_API int mk_search_both(mk_job* job, const mk_search_config* cfg, uint32_t cpu_threads, uint64_t cpu_first,
+                          mk_progress_fn progress, void* user, mk_outcome* out, uint32_t* winner);
+
 /* Continuous batching of many jobs over one candidate stream (no counterpart in the
  * reference): every mk_server_tick is one launch over the next iters_per_tick·keys_per_iter
  * indices of the stream (key, seed source) that tests the needles of all admitted jobs.

@@ -6,7 +6,7 @@ multi-needle matching; the host confirms every hit.  See include/meikey_b200.h.
 """
 from ._lib import (MODE_CONTAINS, MODE_REGEX, MODE_SUFFIX, SEED_CHACHA20, SEED_COUNTER,  # noqa: F401
                    SEED_INCREMENTAL)
-from .engine import Context, GpuError, Graph, Job, Needle, Server  # noqa: F401
+from .engine import Context, GpuError, Graph, Job, Needle, Server, search_many  # noqa: F401
 
-__all__ = ["Context", "Job", "Graph", "Server", "Needle", "GpuError", "SEED_CHACHA20", "SEED_COUNTER", "SEED_INCREMENTAL", "MODE_CONTAINS",
+__all__ = ["Context", "Job", "Graph", "Server", "Needle", "GpuError", "search_many", "SEED_CHACHA20", "SEED_COUNTER", "SEED_INCREMENTAL", "MODE_CONTAINS",
            "MODE_SUFFIX", "MODE_REGEX"]

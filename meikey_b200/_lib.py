@@ -168,6 +168,11 @@ SIGNATURES = [
     ("mk_expected_tries", ctypes.c_double, [ctypes.POINTER(NeedleC)]),
     ("mk_search", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(SearchConfigC), PROGRESS_FN, ctypes.c_void_p,
                                  ctypes.POINTER(OutcomeC)]),
+    ("mk_search_many", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, PROGRESS_FN, ctypes.c_void_p,
+                                      ctypes.POINTER(OutcomeC), ctypes.POINTER(ctypes.c_uint32)]),
+    ("mk_search_both", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(SearchConfigC), ctypes.c_uint32, ctypes.c_uint64,
+                                      PROGRESS_FN, ctypes.c_void_p, ctypes.POINTER(OutcomeC),
+                                      ctypes.POINTER(ctypes.c_uint32)]),
     ("mk_server_create", ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(ServerOptionsC),
                                         ctypes.c_uint64, ctypes.POINTER(ctypes.c_void_p)]),
     ("mk_server_submit", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(NeedleC), ctypes.c_uint64]),

@@ -21,6 +21,7 @@
 #include "abi_guard.h"
 #include "hitsort.h"
 #include "host25519.h"
+#include "jobs.h"
 #include "kernels.h"
 
 using mkb::CombGeom;
@@ -206,6 +207,28 @@ int self_check(mk_ctx* c) {
 }
 
 }  // namespace
+
+namespace mkjobs {
+
+mk_ctx* context_of(const mk_job* job) { return job ? job->ctx : nullptr; }
+
+int host_match(const mk_job* j, uint64_t index, uint8_t pk[32], uint8_t secret[32], uint32_t* needle) {
+    if (j->source == MK_SEED_INCREMENTAL) {
+        if (!mkh25519::incremental_scalar(j->key, index, secret)) return -1;
+        mkh25519::scalar_public_key(secret, pk);
+    } else {
+        mkh25519::seed_of(j->key, j->source, index, secret);
+        mkh25519::public_key(secret, pk);
+    }
+    for (uint32_t k = 0; k < j->needles.size(); k++)
+        if (mkh25519::matches(j->needles[k], pk)) {
+            *needle = k;
+            return 1;
+        }
+    return 0;
+}
+
+}  // namespace mkjobs
 
 extern "C" {
 

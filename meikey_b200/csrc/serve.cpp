@@ -19,17 +19,23 @@
 #include <string.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
+#include <condition_variable>
 #include <deque>
+#include <functional>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <set>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/meikey_b200.h"
 #include "abi_guard.h"
 #include "hitsort.h"
+#include "jobs.h"
 
 namespace {
 
@@ -105,9 +111,22 @@ extern "C" double mk_expected_tries(const mk_needle* nd) try {
     return 0.0;
 }
 
-extern "C" int mk_search(mk_job* job, const mk_search_config* cfg, mk_progress_fn progress, void* user,
-                         mk_outcome* out) try {
-    if (!job || !cfg || !out || cfg->iters == 0) return MK_ERR_BAD_ARG;
+namespace {
+
+// What stops a search loop from outside: the combinators' shared flag (a key was found by
+// another searcher, or the caller cancelled), and the searched indices reported as they grow.
+struct Shared {
+    std::atomic<int>* cancel = nullptr;
+    std::atomic<uint64_t>* tries = nullptr;
+};
+
+// The loop of Searcher::run over one job (src/service/gpu.rs:917-996): launches of cfg->iters
+// iterations over cfg->first, first + keys_per_iter·iters, ...; after each launch its
+// candidates are confirmed on the host in index order and the first that matches with its
+// real x sign ends the search.  A set `cancel` ends it before the next launch, and a launch
+// it cut short (the job's stop word) is not confirmed and not counted.
+int search_loop(mk_job* job, const mk_search_config* cfg, mk_progress_fn progress, void* user, mk_outcome* out,
+                const Shared& sh) {
     memset(out, 0, sizeof *out);
     const double t0 = now_s();
     const uint64_t kpi = mk_job_keys_per_iter(job);
@@ -116,7 +135,12 @@ extern "C" int mk_search(mk_job* job, const mk_search_config* cfg, mk_progress_f
     const uint64_t end = (cfg->max_tries && cfg->max_tries <= ~0ull - cfg->first) ? cfg->first + cfg->max_tries : ~0ull;
     uint64_t base = cfg->first;
     std::vector<mk_hit> hits;
+    auto cancelled = [&] { return sh.cancel && sh.cancel->load() != 0; };
     for (;;) {
+        if (cancelled()) {
+            out->status = MK_ERR_STOPPED;
+            return MK_OK;
+        }
         const uint64_t left = end - base;  // > 0 here
         const uint64_t want = left / kpi + (left % kpi != 0);
         uint32_t iters = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(cfg->iters, want));
@@ -130,6 +154,11 @@ extern "C" int mk_search(mk_job* job, const mk_search_config* cfg, mk_progress_f
             st = mk_job_launch(job, base, iters, &found, &lowest);
         }
         if (st != MK_OK && st != MK_ERR_STOPPED) return st;
+        if (cancelled()) {
+            out->status = MK_ERR_STOPPED;
+            out->elapsed_s = now_s() - t0;
+            return MK_OK;
+        }
         const uint64_t span = kpi * iters;
         if (found) {
             if (int e = fetch_hits(job, hits)) return e;
@@ -146,13 +175,16 @@ extern "C" int mk_search(mk_job* job, const mk_search_config* cfg, mk_progress_f
                     out->needle = h.needle;
                     out->tries = h.index - cfg->first + 1;
                     out->elapsed_s = now_s() - t0;
+                    if (sh.tries) sh.tries->fetch_add(h.index - base + 1);
                     return MK_OK;
                 }
             }
         }
         const bool wrapped = base + span < base;
-        base = wrapped ? end : base + span;
-        out->tries = std::min(base, end) - cfg->first;
+        const uint64_t next = wrapped ? end : std::min(base + span, end);
+        if (sh.tries) sh.tries->fetch_add(next - base);
+        base = next;
+        out->tries = base - cfg->first;
         out->elapsed_s = now_s() - t0;
         if (base >= end) {
             out->status = MK_ERR_STOPPED;  // budget spent without a confirmed key
@@ -167,6 +199,186 @@ extern "C" int mk_search(mk_job* job, const mk_search_config* cfg, mk_progress_f
             return MK_OK;
         }
     }
+}
+
+// Runs `workers` (each returns a status and reports its tries into `tries`) on host threads
+// of their own while the calling thread reports progress about every 100 ms (summed tries);
+// a nonzero progress return, or the time limit, sets `cancel` and calls `stop_all`.  Returns
+// the first worker error, MK_ERR_OUT_OF_MEMORY when a host thread could not start.
+int run_workers(std::vector<std::function<int()>>& workers, std::atomic<int>& cancel, std::atomic<uint64_t>& tries,
+                const std::function<void()>& stop_all, mk_progress_fn progress, void* user, double time_limit_s,
+                double t0) {
+    const size_t n = workers.size();
+    std::vector<int> status(n, MK_OK);
+    std::atomic<size_t> running{n};
+    std::mutex mu;
+    std::condition_variable cv;
+    std::vector<std::thread> threads;
+    bool started_all = true;
+    try {
+        threads.reserve(n);
+        for (size_t k = 0; k < n; k++)
+            threads.emplace_back([&, k] {
+                int st = MK_OK;
+                try {
+                    st = workers[k]();
+                } catch (...) {
+                    st = mkabi::host_failure(nullptr);
+                }
+                status[k] = st;
+                if (st != MK_OK && cancel.exchange(1) == 0) stop_all();
+                std::lock_guard<std::mutex> lock(mu);
+                running--;
+                cv.notify_all();
+            });
+    } catch (...) {
+        started_all = false;  // the host would not start another thread
+        running -= n - threads.size();
+        if (cancel.exchange(1) == 0) stop_all();
+    }
+    {
+        std::unique_lock<std::mutex> lock(mu);
+        while (running.load() > 0) {
+            cv.wait_for(lock, std::chrono::milliseconds(100));
+            if (running.load() == 0 || cancel.load()) continue;
+            const double el = now_s() - t0;
+            lock.unlock();
+            const bool stop = (progress && progress(user, tries.load(), el)) || (time_limit_s > 0 && el >= time_limit_s);
+            if (stop && cancel.exchange(1) == 0) stop_all();
+            lock.lock();
+        }
+    }
+    for (auto& t : threads) t.join();
+    if (!started_all) return MK_ERR_OUT_OF_MEMORY;
+    for (int st : status)
+        if (st != MK_OK) return st;
+    return MK_OK;
+}
+
+}  // namespace
+
+extern "C" int mk_search(mk_job* job, const mk_search_config* cfg, mk_progress_fn progress, void* user,
+                         mk_outcome* out) try {
+    if (!job || !cfg || !out || cfg->iters == 0) return MK_ERR_BAD_ARG;
+    return search_loop(job, cfg, progress, user, out, Shared{});
+} MK_ABI_CATCH(nullptr)
+
+extern "C" int mk_search_many(mk_job* const* jobs, uint32_t n, const mk_search_config* cfgs, mk_progress_fn progress,
+                              void* user, mk_outcome* out, uint32_t* winner) try {
+    if (!jobs || !cfgs || !out || !winner || n == 0 || n > 64) return MK_ERR_BAD_ARG;
+    for (uint32_t k = 0; k < n; k++) {
+        if (!jobs[k] || cfgs[k].iters == 0) return MK_ERR_BAD_ARG;
+        for (uint32_t q = 0; q < k; q++)  // one host thread per context
+            if (mkjobs::context_of(jobs[q]) == mkjobs::context_of(jobs[k])) return MK_ERR_BAD_ARG;
+    }
+    memset(out, 0, sizeof *out);
+    *winner = n;
+    const double t0 = now_s();
+    std::atomic<int> cancel{0};
+    std::atomic<uint64_t> tries{0};
+    std::atomic<uint32_t> first_found{n};
+    std::vector<mk_outcome> outs(n);
+    auto stop_all = [&] {
+        for (uint32_t q = 0; q < n; q++) mk_job_stop(jobs[q], 1);
+    };
+    std::vector<std::function<int()>> workers;
+    for (uint32_t k = 0; k < n; k++)
+        workers.push_back([&, k] {
+            // the calling thread reports progress; the time limit is checked there too
+            mk_search_config cfg = cfgs[k];
+            cfg.time_limit_s = 0;
+            int st = search_loop(jobs[k], &cfg, nullptr, nullptr, &outs[k], Shared{&cancel, &tries});
+            if (st == MK_OK && outs[k].status == MK_OK) {
+                uint32_t none = n;
+                if (first_found.compare_exchange_strong(none, k)) {
+                    cancel.store(1);
+                    for (uint32_t q = 0; q < n; q++)
+                        if (q != k) mk_job_stop(jobs[q], 1);
+                }
+            }
+            return st;
+        });
+    int st = run_workers(workers, cancel, tries, stop_all, progress, user, cfgs[0].time_limit_s, t0);
+    for (uint32_t q = 0; q < n; q++) mk_job_stop(jobs[q], 0);  // withdraw the stop requests
+    const uint32_t w = first_found.load();
+    if (w < n) {
+        *out = outs[w];
+        *winner = w;
+    } else {
+        out->status = MK_ERR_STOPPED;
+    }
+    out->tries = tries.load();
+    out->elapsed_s = now_s() - t0;
+    return st;
+} MK_ABI_CATCH(nullptr)
+
+extern "C" int mk_search_both(mk_job* job, const mk_search_config* cfg, uint32_t cpu_threads, uint64_t cpu_first,
+                              mk_progress_fn progress, void* user, mk_outcome* out, uint32_t* winner) try {
+    if (!job || !cfg || !out || !winner || cfg->iters == 0 || cpu_threads > 256) return MK_ERR_BAD_ARG;
+    memset(out, 0, sizeof *out);
+    *winner = 2;
+    const double t0 = now_s();
+    std::atomic<int> cancel{0};
+    std::atomic<uint64_t> tries{0}, next_cpu{cpu_first};
+    std::atomic<uint32_t> first_found{2};
+    mk_outcome gpu_out{}, cpu_out{};
+    std::mutex cpu_mu;
+    auto stop_all = [&] { mk_job_stop(job, 1); };
+    auto claim = [&](uint32_t who) {
+        uint32_t none = 2;
+        if (!first_found.compare_exchange_strong(none, who)) return false;
+        cancel.store(1);
+        if (who == 1) mk_job_stop(job, 1);
+        return true;
+    };
+    std::vector<std::function<int()>> workers;
+    workers.push_back([&] {
+        mk_search_config c = *cfg;
+        c.time_limit_s = 0;
+        int st = search_loop(job, &c, nullptr, nullptr, &gpu_out, Shared{&cancel, &tries});
+        if (st == MK_OK && gpu_out.status == MK_OK) claim(0);
+        return st;
+    });
+    // CPU searchers: chunks of consecutive indices from cpu_first, the host derivation and a
+    // full match (x sign known), the reference's Parallel worker (src/service/search.rs:195-317)
+    const uint64_t CHUNK = 64;
+    for (uint32_t t = 0; t < cpu_threads; t++)
+        workers.push_back([&] {
+            uint8_t pk[32], secret[32];
+            while (!cancel.load()) {
+                const uint64_t a = next_cpu.fetch_add(CHUNK);
+                for (uint64_t i = a; i < a + CHUNK; i++) {
+                    uint32_t needle = 0;
+                    const int m = mkjobs::host_match(job, i, pk, secret, &needle);
+                    if (m < 0) return (int)MK_ERR_BAD_ARG;
+                    if (m == 1) {
+                        tries.fetch_add(i - a + 1);
+                        std::lock_guard<std::mutex> lock(cpu_mu);
+                        if (first_found.load() == 2 && (cpu_out.status != MK_OK || i < cpu_out.index)) {
+                            cpu_out.status = MK_OK;
+                            cpu_out.index = i;
+                            cpu_out.needle = needle;
+                            memcpy(cpu_out.pk, pk, 32);
+                            memcpy(cpu_out.secret, secret, 32);
+                        }
+                        claim(1);
+                        return (int)MK_OK;
+                    }
+                }
+                tries.fetch_add(CHUNK);
+            }
+            return (int)MK_OK;
+        });
+    int st = run_workers(workers, cancel, tries, stop_all, progress, user, cfg->time_limit_s, t0);
+    mk_job_stop(job, 0);
+    const uint32_t w = first_found.load();
+    if (w == 0) *out = gpu_out;
+    else if (w == 1) *out = cpu_out;
+    else out->status = MK_ERR_STOPPED;
+    *winner = w;
+    out->tries = tries.load();
+    out->elapsed_s = now_s() - t0;
+    return st;
 } MK_ABI_CATCH(nullptr)
 
 // ---------------------------------------------------------------------------

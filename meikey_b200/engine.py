@@ -67,6 +67,34 @@ class Needle:
         return float(L.load().mk_expected_tries(arr))
 
 
+def _outcome(out) -> dict:
+    return {"status": out.status, "found": out.status == L.OK, "index": int(out.index), "needle": int(out.needle),
+            "tries": int(out.tries), "elapsed_s": float(out.elapsed_s), "secret": bytes(out.secret),
+            "pk": bytes(out.pk)}
+
+
+def _progress_fn(progress):
+    return L.PROGRESS_FN((lambda user, tries, el: 1 if progress(int(tries), float(el)) else 0)
+                         if progress else (lambda user, tries, el: 0))
+
+
+def search_many(jobs, first, max_tries=0, iters=16, time_limit_s=0.0, progress=None) -> dict:
+    """Searcher::run over several jobs, one host thread each (mk_search_many, the reference's
+    All): `first` and `max_tries` are one value for all jobs or one per job; the first key
+    found stops the others.  Returns the winner's outcome with `winner` (len(jobs): none)."""
+    n = len(jobs)
+    firsts = first if isinstance(first, (list, tuple)) else [first] * n
+    budgets = max_tries if isinstance(max_tries, (list, tuple)) else [max_tries] * n
+    cfgs = (L.SearchConfigC * n)(*[L.SearchConfigC(f, m, time_limit_s, iters, 0) for f, m in zip(firsts, budgets)])
+    ptrs = (ctypes.c_void_p * n)(*[j._ptr.value for j in jobs])
+    out = L.OutcomeC()
+    who = ctypes.c_uint32()
+    lib = jobs[0]._lib
+    _check(lib, jobs[0].ctx._ptr, lib.mk_search_many(ptrs, n, cfgs, _progress_fn(progress), None, ctypes.byref(out),
+                                                     ctypes.byref(who)))
+    return dict(_outcome(out), winner=int(who.value))
+
+
 def _check(lib, ctx_ptr, status: int):
     if status != L.OK:
         buf = ctypes.create_string_buffer(512)
@@ -244,6 +272,18 @@ class Job:
         return {"status": out.status, "found": out.status == L.OK, "index": int(out.index), "needle": int(out.needle),
                 "tries": int(out.tries), "elapsed_s": float(out.elapsed_s), "secret": bytes(out.secret),
                 "pk": bytes(out.pk)}
+
+    def search_both(self, first: int = 0, max_tries: int = 0, iters: int = 16, time_limit_s: float = 0.0,
+                    cpu_threads: int = 1, cpu_first: int = 1 << 62, progress=None) -> dict:
+        """The GPU and `cpu_threads` host threads searching together (mk_search_both, the
+        reference's Both): the first key either side finds; `winner` 0 GPU, 1 host, 2 none."""
+        cfg = L.SearchConfigC(first, max_tries, time_limit_s, iters, 0)
+        out = L.OutcomeC()
+        who = ctypes.c_uint32()
+        cb = _progress_fn(progress)
+        _check(self._lib, self.ctx._ptr, self._lib.mk_search_both(self._ptr, ctypes.byref(cfg), cpu_threads, cpu_first,
+                                                                  cb, None, ctypes.byref(out), ctypes.byref(who)))
+        return dict(_outcome(out), winner=int(who.value))
 
     def stop(self, on: bool = True):
         """Request (or withdraw) a stop of this job's launches, also of one that is running."""
