@@ -610,6 +610,7 @@ def measure(args, workload, steps, e2e_steps, dist, world, rank, local, cpu_seco
     step_keys = kpi * iters * launches
     rank_base = rank_first(rank, 0, step_keys)
     peak, peak_lo = ctx.measure_mad_peaks()
+    pieces = ctx.measure_imad_rates() if workload == args.workload else None
     field_muls, mads_per_key = ctx.work_per_key(source)
     needles = workload_needles(workload)
     job = ctx.job(key, source, needles)
@@ -697,6 +698,8 @@ def measure(args, workload, steps, e2e_steps, dist, world, rank, local, cpu_seco
             "peak_mad_lo": peak_lo / 1e12,
             "frac_of_mad_lo": achieved / (peak_lo / 1e12) if peak_lo else None,
             "work_per_key": {"field_muls": field_muls, "int_mads": mads_per_key},
+            # the peak's pieces, each on independent chains or carry-linked rows (Tmad/s)
+            "imad_pieces": {k: v / 1e12 for k, v in pieces.items()} if pieces else None,
             "kernel_ms_per_launch": ms_local / (steps * launches),
         }
         cfg = workload_config(workload, ctx, step_keys, steps)

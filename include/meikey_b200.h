@@ -69,9 +69,10 @@ enum mk_mode { MK_MODE_CONTAINS = 0, MK_MODE_SUFFIX = 1, MK_MODE_REGEX = 2 };
  * table_rows chooses the comb geometry (rows of the fixed-base table: fewer rows
  * means fewer point additions per key and a larger table in HBM). */
 typedef struct mk_options {
-    uint32_t table_rows;      /* 10..20; default 12 */
+    uint32_t table_rows;      /* 10..63; default 12 (rows 10-20 are HBM tables of 26 GB down to 11 MB, 32-63 the
+                                 comb windows of 8 down to 4 bits) */
     uint32_t keys_per_thread; /* keys one thread derives before the pooled inversion (default 16) */
-    uint32_t block;           /* threads per CTA (default 512): 256 (keys per thread 4, 8, 16) or 512 (8, 16);
+    uint32_t block;           /* threads per CTA (default 512): 256 or 512, keys per thread 4, 8 or 16;
                                  see inverter_rotates for who inverts */
     uint32_t blocks_per_sm;   /* resident CTAs per SM the grid is sized for (0 = occupancy maximum) */
     uint32_t self_check;      /* 1: derive keys at creation and compare with the host derivation */
@@ -89,6 +90,11 @@ typedef struct mk_options {
                                  at most 32, e.g. 256 = 8 x 480 / 15.  0: 32 pools (keys_per_thread x 15,
                                  x 16 with inverter_rotates, x 11 with hash_warps); else
                                  MK_ERR_OUT_OF_RANGE when no pool count gives it */
+    uint32_t table_in_smem;   /* 1: every search CTA copies the comb table into shared memory and reads its
+                                 entries there instead of gathering them from HBM (96 bytes an entry: about
+                                 40+ rows, e.g. 42 rows of 6-bit digits, 133 KB; block 512, keys per thread
+                                 4 or 8, the dedicated inverter; regex tables then stay in global memory).
+                                 MK_ERR_OUT_OF_RANGE when the table does not fit */
 } mk_options;
 
 /* One pattern as the reference's GPU needle (Needle, src/service/gpu.rs:618-660):
@@ -123,7 +129,7 @@ typedef struct mk_info {
     uint64_t keys_per_iter;   /* grid · (block - 32; block with inverter_rotates; 352 with hash_warps) · keys_per_thread */
     char name[96];
     uint32_t inversion_batch; /* keys sharing one field inversion */
-    uint32_t reserved;
+    uint32_t table_in_smem;   /* 1: search CTAs read the comb table from shared memory */
 } mk_info;
 
 /* One candidate of the autotuner and what it measured. */
@@ -437,6 +443,14 @@ MK_API int mk_ctx_work_per_key(const mk_ctx* ctx, int seed_source, double* field
  *   *lo_per_s     plain mad.lo.u32 on independent registers (the low-half multiply rate).
  * The reference reports no roofline. */
 MK_API int mk_measure_mad_peaks(mk_ctx* ctx, double* chain_per_s, double* lo_per_s);
+
+/* The pieces of that instruction shape, each on 8 independent chains per thread at full
+ * occupancy (multiply-adds per second): independent mad.hi.u32, independent mad.wide.u32
+ * (a full 64-bit product into a 64-bit sum), and rows of 8 madc.lo.cc or 8 madc.hi.cc linked
+ * through the carry flag.  Together with mk_measure_mad_peaks they separate the issue cost of
+ * the high halves from the serialisation of the carry chains. */
+MK_API int mk_measure_imad_rates(mk_ctx* ctx, double* hi_per_s, double* wide_per_s, double* lo_chain_per_s,
+                                 double* hi_chain_per_s);
 
 #ifdef __cplusplus
 }

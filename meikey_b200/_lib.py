@@ -50,6 +50,7 @@ class Options(ctypes.Structure):
         ("hash_warps", ctypes.c_uint32),
         ("inverter_rotates", ctypes.c_uint32),
         ("inversion_batch", ctypes.c_uint32),
+        ("table_in_smem", ctypes.c_uint32),
     ]
 
 
@@ -108,7 +109,7 @@ class InfoC(ctypes.Structure):
         ("keys_per_iter", ctypes.c_uint64),
         ("name", ctypes.c_char * 96),
         ("inversion_batch", ctypes.c_uint32),
-        ("reserved", ctypes.c_uint32),
+        ("table_in_smem", ctypes.c_uint32),
     ]
 
 
@@ -149,6 +150,7 @@ SIGNATURES = [
                                        ctypes.POINTER(ctypes.c_uint64)]),
     ("mk_ctx_work_per_key", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
                                            ctypes.POINTER(ctypes.c_double)]),
+    ("mk_measure_imad_rates", ctypes.c_int, [ctypes.c_void_p] + [ctypes.POINTER(ctypes.c_double)] * 4),
     ("mk_measure_mad_peaks", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
                                             ctypes.POINTER(ctypes.c_double)]),
     ("mk_regex_compile", ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_uint32, ctypes.c_void_p,

@@ -42,6 +42,7 @@ struct mk_ctx {
     uint32_t hash_warps = 0;  // 4: search kernel with hashing warps (ChaCha20 / counter seeds)
     uint32_t layout = mkb::LAYOUT_INVERTER_WARP;  // division of work inside a search CTA
     uint32_t inv_pools = 32;  // field inversions per search CTA and iteration
+    uint32_t table_smem = 0;  // bytes of the comb table each search CTA keeps in shared memory (0: HBM)
     uint32_t hit_capacity = 1u << 16;
     uint8_t* noalloc = nullptr;  // device address of mk_derive_noalloc's fixed staging array
     std::string err;
@@ -261,10 +262,14 @@ int mk_ctx_create(int device, const mk_options* options, mk_ctx** out) try {
     if (!o.keys_per_thread) o.keys_per_thread = 16;
     if (!o.block) o.block = 512;
     const bool built = (o.block == 256 && (o.keys_per_thread == 4 || o.keys_per_thread == 8 || o.keys_per_thread == 16)) ||
-                       (o.block == 512 && (o.keys_per_thread == 8 || o.keys_per_thread == 16));
+                       (o.block == 512 && (o.keys_per_thread == 4 || o.keys_per_thread == 8 || o.keys_per_thread == 16));
+    // the shared-memory table: built for the dedicated-inverter layout, block 512, 4 or 8 keys per thread
+    const bool smem_ok = o.table_in_smem == 0 ||
+                         (o.table_in_smem == 1 && o.block == 512 && (o.keys_per_thread == 4 || o.keys_per_thread == 8) &&
+                          !o.hash_warps && !o.inverter_rotates);
     const bool hw_ok = o.hash_warps == 0 || (o.hash_warps == 4 && o.block == 512 && (o.keys_per_thread == 8 || o.keys_per_thread == 16));
     const bool rot_ok = o.inverter_rotates <= 1 && !(o.inverter_rotates && o.hash_warps);
-    if (o.table_rows < 10 || o.table_rows > (uint32_t)mkb::MAX_ROWS || !built || !hw_ok || !rot_ok ||
+    if (o.table_rows < 10 || o.table_rows > (uint32_t)mkb::MAX_ROWS - 1 || !built || !hw_ok || !rot_ok || !smem_ok ||
         o.blocks_per_sm > 16 || o.hit_capacity > (1u << 26))
         return MK_ERR_OUT_OF_RANGE;
     // inversion batch: keys per field inversion = keys per thread x compute threads / pools, with
@@ -307,12 +312,23 @@ int mk_ctx_create(int device, const mk_options* options, mk_ctx** out) try {
     for (auto& ev : c->ev) MK_CUDA(c, cudaEventCreate(&ev));
     cudaDeviceProp prop;
     MK_CUDA(c, cudaGetDeviceProperties(&prop, device));
+    if (!make_geometry(o.table_rows, c->geom)) return fail(c, MK_ERR_OUT_OF_RANGE, "no comb geometry for this row count");
+    if (o.table_in_smem) {
+        const uint64_t bytes = c->geom.entries * (uint64_t)mkb::ENTRY_WORDS * 4;  // 96 bytes per entry
+        if (bytes > (uint64_t)prop.sharedMemPerBlockOptin)
+            return fail(c, MK_ERR_OUT_OF_RANGE, "the comb table does not fit in shared memory (use more rows)");
+        c->table_smem = (uint32_t)bytes;
+    }
     int occ = 0;
-    MK_CUDA(c, mkb::keys_occupancy(false, false, c->kpt, c->block, c->layout, &occ));
+    cudaError_t oe = mkb::keys_occupancy(false, false, c->kpt, c->block, c->layout, c->table_smem, &occ);
+    if (oe != cudaSuccess && c->table_smem) {
+        cudaGetLastError();
+        return fail(c, MK_ERR_OUT_OF_RANGE, "the comb table and the CTA's buffers do not fit in shared memory");
+    }
+    MK_CUDA(c, oe);
     if (occ < 1) return fail(c, MK_ERR_NOT_BUILT, "kernel does not fit on this device");
     uint32_t per_sm = o.blocks_per_sm ? std::min<uint32_t>(o.blocks_per_sm, (uint32_t)occ) : (uint32_t)occ;
     c->grid = (uint32_t)prop.multiProcessorCount * per_sm;
-    if (!make_geometry(o.table_rows, c->geom)) return fail(c, MK_ERR_OUT_OF_RANGE, "no comb geometry for this row count");
     // table
     size_t bytes = (size_t)c->geom.entries * mkb::COMB_STRIDE_WORDS * 4;
     e = cudaMalloc(&c->table, bytes);
@@ -360,6 +376,7 @@ int mk_ctx_create(int device, const mk_options* options, mk_ctx** out) try {
     // inversion rotates; 352 comb threads with hashing warps)
     in.keys_per_iter = (uint64_t)c->grid * mkb::search_threads(c->block, c->layout) * c->kpt;
     in.inversion_batch = mkb::search_threads(c->block, c->layout) * c->kpt / c->inv_pools;
+    in.table_in_smem = c->table_smem ? 1 : 0;
     snprintf(in.name, sizeof in.name, "%.95s", prop.name);
     if (o.self_check) {
         int st = self_check(c);
@@ -721,6 +738,7 @@ void mk_job_destroy(mk_job* j) try {
 // Shared memory for the job's DFA tables when they fit (the kernel then reads them there).
 static uint32_t dfa_smem_bytes(const mk_job* j) {
     if (j->ctx->hash_warps) return 0;  // the hashing-warp kernel's scalar ring takes that shared memory
+    if (j->ctx->table_smem) return 0;  // so does a comb table kept in shared memory
     uint64_t total = 0;
     for (const auto& h : j->needles)
         if (h.mode == MK_MODE_REGEX) total += ((uint64_t)h.len * 130 + 15) & ~15ull;
@@ -748,6 +766,7 @@ static mkb::KeyLaunch search_params(const mk_job* j, uint64_t base, uint32_t ite
     L.dfa_smem = dfa_smem_bytes(j);
     L.layout = c->layout;
     L.inv_pools = c->inv_pools;
+    L.table_smem = c->table_smem;
     return L;
 }
 
@@ -978,6 +997,19 @@ int mk_ctx_work_per_key(const mk_ctx* c, int seed_source, double* field_muls, do
     return MK_OK;
 }
 
+int mk_measure_imad_rates(mk_ctx* c, double* hi_per_s, double* wide_per_s, double* lo_chain_per_s,
+                          double* hi_chain_per_s) try {
+    if (!c || !hi_per_s || !wide_per_s || !lo_chain_per_s || !hi_chain_per_s) return MK_ERR_BAD_ARG;
+    MK_CUDA(c, cudaSetDevice(c->device));
+    double r[4] = {0, 0, 0, 0};
+    MK_CUDA(c, mkb::measure_imad_rates((int)c->info.sms, c->stream, r));
+    *hi_per_s = r[0];
+    *wide_per_s = r[1];
+    *lo_chain_per_s = r[2];
+    *hi_chain_per_s = r[3];
+    return MK_OK;
+} MK_ABI_CATCH(c ? &c->err : nullptr)
+
 int mk_measure_mad_peaks(mk_ctx* c, double* chain_per_s, double* lo_per_s) try {
     if (!c || !chain_per_s || !lo_per_s) return MK_ERR_BAD_ARG;
     MK_CUDA(c, cudaSetDevice(c->device));
@@ -1019,7 +1051,7 @@ int mk_job_graph_create(mk_job* j, uint32_t iters, uint32_t launches, mk_graph**
     const void* func = nullptr;
     size_t dyn = 0;
     e = mkb::keys_kernel(false, j->source == MK_SEED_INCREMENTAL, c->kpt, c->block, c->layout, dfa_smem_bytes(j),
-                         &func, &dyn);
+                         c->table_smem, &func, &dyn);
     if (e != cudaSuccess) return bail(e, "keys_kernel");
     for (uint32_t i = 0; i < launches; i++) {
         g->params[i] = search_params(j, g->span * i, iters);
@@ -1048,7 +1080,8 @@ static int graph_enqueue(mk_graph* g, uint64_t base) {
     mk_ctx* c = j->ctx;
     MK_CUDA(c, cudaSetDevice(c->device));
     // the job's needles may have changed since the graph was made: size the DFA staging anew
-    MK_CUDA(c, mkb::keys_kernel(false, j->source == MK_SEED_INCREMENTAL, c->kpt, c->block, c->layout, dfa_smem_bytes(j), &g->func,
+    MK_CUDA(c, mkb::keys_kernel(false, j->source == MK_SEED_INCREMENTAL, c->kpt, c->block, c->layout, dfa_smem_bytes(j),
+                                c->table_smem, &g->func,
                                 &g->dyn));
     for (size_t i = 0; i < g->nodes.size(); i++) {
         g->params[i] = search_params(j, base + g->span * i, g->iters);

@@ -156,36 +156,42 @@ __device__ __forceinline__ u64 entry_index(const CombGeom& g, u32 row, int d) {
     return g.row_base[row] + (u64)(d < 0 ? -d : d);
 }
 
-// Comb multiply: s (clamped, 4 LE words) -> y = yn/yd (and x = xn/xd when wanted).
-// Row r's entry is fetched while row r-1 is being added.
-__device__ __forceinline__ void comb_mul(const uint4* __restrict__ table, const CombGeom& g, const u64 s[4],
-                                         EntrySlot& slot, fe& yn, fe& yd, fe* xn, fe* xd) {
-    // m = bits 3..253 of s
-    u64 m[4];
+// bits 3..253 of a clamped scalar s: the number whose digits the comb rows take
+__device__ __forceinline__ void comb_m(const u64 s[4], u64 m[4]) {
     m[0] = s[0] >> 3 | s[1] << 61;
     m[1] = s[1] >> 3 | s[2] << 61;
     m[2] = s[2] >> 3 | s[3] << 61;
     m[3] = (s[3] >> 3) & ((1ull << (251 - 192)) - 1ull);
+}
+
+// Row 0's entry (digit sign `neg`) in extended coordinates: X = 2x, Y = 2y, Z = 2, T = 2xy,
+// without a multiplication (row 0 stores 2xy).
+__device__ __forceinline__ ge comb_row0(niels n, bool neg) {
+    ge P;
+    mk32::fe_cswap(n.ypx, n.ymx, neg);
+    P.X = mk32::fe_sub(n.ypx, n.ymx);
+    P.Y = mk32::fe_add(n.ypx, n.ymx);
+    P.Z = mk32::fe_small(2);
+    fe nt = mk32::fe_sub(mk32::fe_zero(), n.t2d);
+#pragma unroll
+    for (int i = 0; i < 8; i++) P.T.v[i] = neg ? nt.v[i] : n.t2d.v[i];
+    return P;
+}
+
+// Comb multiply: s (clamped, 4 LE words) -> y = yn/yd (and x = xn/xd when wanted).
+// Row r's entry is fetched while row r-1 is being added.
+__device__ __forceinline__ void comb_mul(const uint4* __restrict__ table, const CombGeom& g, const u64 s[4],
+                                         EntrySlot& slot, fe& yn, fe& yd, fe* xn, fe* xd) {
+    u64 m[4];
+    comb_m(s, m);
     const u32 rows = g.rows;
     int carry = 0;
     int d0 = next_digit(g, m, 0, carry);
     fetch_entry(slot, 0, table, entry_index(g, 0, d0));
     int dn = next_digit(g, m, 1, carry);  // rows >= 3, so row 1 is not the top row
     fetch_entry(slot, 1, table, entry_index(g, 1, dn));
-    // row 0 -> extended coordinates (X = 2x, Y = 2y, Z = 2, T = 2xy)
     wait_entries<1>();
-    ge P;
-    {
-        niels n = read_entry(slot, 0);
-        const bool neg = d0 < 0;
-        mk32::fe_cswap(n.ypx, n.ymx, neg);
-        P.X = mk32::fe_sub(n.ypx, n.ymx);
-        P.Y = mk32::fe_add(n.ypx, n.ymx);
-        P.Z = mk32::fe_small(2);
-        fe nt = mk32::fe_sub(mk32::fe_zero(), n.t2d);
-#pragma unroll
-        for (int i = 0; i < 8; i++) P.T.v[i] = neg ? nt.v[i] : n.t2d.v[i];
-    }
+    ge P = comb_row0(read_entry(slot, 0), d0 < 0);
 #pragma unroll 1
     for (u32 row = 1; row + 1 < rows; row++) {
         const int d = dn;
@@ -389,15 +395,38 @@ __device__ __forceinline__ void scalars(const KeyLaunch& L, const u32 key[8], co
     for (int j = 0; j < KPT; j++) scalar_of(L.seed_src, key, mid, first + (u64)j, blk, blk_id, sc[j]);
 }
 
-// Comb multiplies of the KPT scalars (IMAD work) into the batch.
-template <int KPT>
+__device__ __forceinline__ niels smem_niels(const uint4* q);
+
+// Comb multiply with the whole table in shared memory (entries 96 bytes apart, `stab`): every
+// row reads its entry there, with no staging; y = yn/yd only.
+__device__ __forceinline__ void comb_mul_smem(const uint4* stab, const CombGeom& g, const u64 s[4], fe& yn, fe& yd) {
+    u64 m[4];
+    comb_m(s, m);
+    const u32 rows = g.rows;
+    int carry = 0;
+    int d = next_digit(g, m, 0, carry);
+    ge P = comb_row0(smem_niels(stab + entry_index(g, 0, d) * 6), d < 0);
+#pragma unroll 1
+    for (u32 row = 1; row + 1 < rows; row++) {
+        d = next_digit(g, m, row, carry);
+        P = mk32::ge_add_niels(P, smem_niels(stab + entry_index(g, row, d) * 6), d < 0);
+    }
+    // the top row's digit is unsigned: the carry lands in it unchanged
+    d = (int)bits_at(m, g.offset[rows - 1], g.width[rows - 1]) + carry;
+    mk32::ge_add_niels_frac(P, smem_niels(stab + entry_index(g, rows - 1, d) * 6), yn, yd, nullptr, nullptr);
+}
+
+// Comb multiplies of the KPT scalars (IMAD work) into the batch; STAB: from the table in
+// shared memory.
+template <int KPT, bool STAB = false>
 __device__ __forceinline__ void combs(const KeyLaunch& L, const CombGeom& g, const u64 sc[KPT][4], EntrySlot& slot,
-                                      Batch<KPT>& b) {
+                                      const uint4* stab, Batch<KPT>& b) {
     fe run;
 #pragma unroll 1
     for (int j = 0; j < KPT; j++) {
         fe num;
-        comb_mul(L.table, g, sc[j], slot, num, b.den[j], nullptr, nullptr);
+        if (STAB) comb_mul_smem(stab, g, sc[j], num, b.den[j]);
+        else comb_mul(L.table, g, sc[j], slot, num, b.den[j], nullptr, nullptr);
         if (j == 0) {
             b.a[0] = num;
             run = b.den[0];
@@ -555,7 +584,9 @@ __device__ __forceinline__ void incr_fracs(const ge& Q, const uint4* steps, Batc
 // INCR: the incremental source.  A compute thread keeps the point Q of its first index in
 // the current iteration; its keys are Q + j·B from the step table, and Q advances by
 // keys_per_iter·B (one mixed addition) per iteration.  No comb table is read.
-template <int KPT, int BLOCK, bool INCR, bool ROT>
+// STAB: the comb table lives in shared memory (copied by every CTA at the start, in place of
+// the staging slots; tables of a few hundred to a few thousand entries, 40+ rows).
+template <int KPT, int BLOCK, bool INCR, bool ROT, bool STAB = false>
 __global__ void __launch_bounds__(BLOCK, 512 / BLOCK) k_search(const KeyLaunch L) {
     constexpr int CT = ROT ? BLOCK : BLOCK - 32;  // compute threads
     constexpr int CW = CT / 32;                   // compute warps
@@ -563,6 +594,7 @@ __global__ void __launch_bounds__(BLOCK, 512 / BLOCK) k_search(const KeyLaunch L
     fe (*prod)[CT] = reinterpret_cast<fe (*)[CT]>(dyn_smem);
     fe (*scratch)[CT] = prod + 2;
     EntrySlot* slots = reinterpret_cast<EntrySlot*>(scratch + 2);
+    uint4* stab = reinterpret_cast<uint4*>(scratch + 2);  // STAB: the table in place of the slots
     __shared__ CombGeom g;
     __shared__ MatchSet ms;
     __shared__ u32 lane_masks[64 * 32];  // see match_key
@@ -583,6 +615,10 @@ __global__ void __launch_bounds__(BLOCK, 512 / BLOCK) k_search(const KeyLaunch L
         if (tid == 0) stop_iter = L.iters;
     }
     __syncthreads();
+    if (STAB)  // entries 128 bytes apart in HBM, 96 here
+        for (u32 e = tid; e < (u32)g.entries; e += BLOCK)
+#pragma unroll
+            for (int q = 0; q < 6; q++) stab[e * 6 + q] = L.table[(u64)e * (COMB_STRIDE_WORDS / 4) + q];
     u32 dfa_need = 0;
     for (u32 r = 0; r < ms.n_regex; r++) dfa_need += (ms.dfa_states[r] * 130u + 15u) & ~15u;
     if (L.dfa_smem && dfa_need <= L.dfa_smem) {
@@ -643,7 +679,7 @@ __global__ void __launch_bounds__(BLOCK, 512 / BLOCK) k_search(const KeyLaunch L
     auto inverts = [&](u32 it) { return ROT && warp == (u32)CW - 4u + (it & 3u); };
     const u64 gid = (u64)blockIdx.x * CT + tid;
     const u64 nthreads = (u64)gridDim.x * CT;
-    EntrySlot& slot = slots[INCR ? 0 : tid];
+    EntrySlot& slot = slots[INCR || STAB ? 0 : tid];
     Batch<KPT> batch[2];
     u64 sc[KPT][4];
     u32 sink = 0;
@@ -657,7 +693,7 @@ __global__ void __launch_bounds__(BLOCK, 512 / BLOCK) k_search(const KeyLaunch L
             Q = mk32::ge_add_niels(Q, words_niels(L.delta), false);
         } else {
             scalars<KPT>(L, key, mid, first_of(it), sc);
-            combs<KPT>(L, g, sc, slot, batch[b]);
+            combs<KPT, STAB>(L, g, sc, slot, stab, batch[b]);
         }
         prod[b][tid] = batch[b].prod;
         if (inverts(it)) {
@@ -945,18 +981,19 @@ __global__ void __launch_bounds__(BLOCK, 512 / BLOCK) k_derive(const KeyLaunch L
 // host launch wrappers
 // ---------------------------------------------------------------------------
 
-#define MK_VARIANTS(X) X(4, 256) X(8, 256) X(16, 256) X(8, 512) X(16, 512)
+#define MK_VARIANTS(X) X(4, 256) X(8, 256) X(16, 256) X(4, 512) X(8, 512) X(16, 512)
 
 // dynamic shared memory: products and inversion scratch (two buffers each for the
 // search pipeline) and the per-thread table staging slots
 // (the incremental source reads no comb table and needs no staging slots)
-static size_t dyn_bytes(bool derive, bool incr, uint32_t block, uint32_t layout) {
+static size_t dyn_bytes(bool derive, bool incr, uint32_t block, uint32_t layout, uint32_t table_smem) {
     const size_t fe_bytes = 32;
     if (layout == LAYOUT_HASH_WARPS && !derive && !incr) {  // k_search_hw: 352 comb threads, plus the two-slot scalar ring
         const size_t ct = 352;
         return 4 * ct * fe_bytes + ct * sizeof(EntrySlot) + 2 * 4 * ct * 32;
     }
     const size_t threads = derive ? block : search_threads(block, layout == LAYOUT_HASH_WARPS ? LAYOUT_INVERTER_WARP : layout);
+    if (table_smem && !derive && !incr) return 4 * threads * fe_bytes + table_smem;  // the table in place of the slots
     return (derive ? 2 : 4) * threads * fe_bytes + (incr ? 0 : threads * sizeof(EntrySlot));
 }
 
@@ -964,6 +1001,15 @@ static const void* hw_kernel_of(uint32_t kpt, uint32_t block) {
     if (block != 512) return nullptr;
     if (kpt == 8) return (const void*)k_search_hw<8, 512>;
     if (kpt == 16) return (const void*)k_search_hw<16, 512>;
+    return nullptr;
+}
+
+// search kernels with the comb table in shared memory: the dedicated-inverter layout, block
+// 512, keys per thread 4 and 8
+static const void* stab_kernel_of(uint32_t kpt, uint32_t block) {
+    if (block != 512) return nullptr;
+    if (kpt == 4) return (const void*)k_search<4, 512, false, false, true>;
+    if (kpt == 8) return (const void*)k_search<8, 512, false, false, true>;
     return nullptr;
 }
 
@@ -983,15 +1029,25 @@ static cudaError_t prepare(const void* f, size_t dyn) {
     return cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
 }
 
+// the kernel of a variant (the table-in-shared-memory search when table_smem > 0)
+static const void* variant_kernel(bool derive, bool incr, uint32_t kpt, uint32_t block, uint32_t layout,
+                                  uint32_t table_smem) {
+    const bool hw = layout == LAYOUT_HASH_WARPS && !derive && !incr;
+    if (table_smem && !derive && !incr) return layout == LAYOUT_INVERTER_WARP ? stab_kernel_of(kpt, block) : nullptr;
+    return hw ? hw_kernel_of(kpt, block) : kernel_of(derive, incr, kpt, block, layout == LAYOUT_ROTATING);
+}
+
 cudaError_t launch_keys(const KeyLaunch& L, bool derive, uint32_t kpt, uint32_t block, uint32_t grid, cudaStream_t st) {
     const bool incr = L.seed_src == SEED_INCREMENTAL;
     if (incr && (kpt > (uint32_t)INCR_STEPS || !L.incr)) return cudaErrorInvalidValue;
     if (L.dfa_smem > DFA_SMEM_MAX || (derive && L.dfa_smem)) return cudaErrorInvalidValue;
     const bool hw = L.layout == LAYOUT_HASH_WARPS && !derive && !incr;
     if (hw && L.dfa_smem) return cudaErrorInvalidValue;  // the scalar ring takes that shared memory
-    const void* f = hw ? hw_kernel_of(kpt, block) : kernel_of(derive, incr, kpt, block, L.layout == LAYOUT_ROTATING);
+    const uint32_t tsm = derive || incr ? 0 : L.table_smem;
+    if (tsm && L.dfa_smem) return cudaErrorInvalidValue;  // the table takes that shared memory
+    const void* f = variant_kernel(derive, incr, kpt, block, L.layout, tsm);
     if (!f) return cudaErrorInvalidValue;
-    const size_t dyn = dyn_bytes(derive, incr, block, L.layout) + L.dfa_smem;
+    const size_t dyn = dyn_bytes(derive, incr, block, L.layout, tsm) + L.dfa_smem;
     cudaError_t e = prepare(f, dyn);
     if (e != cudaSuccess) return e;
     void* args[] = {const_cast<KeyLaunch*>(&L)};
@@ -999,20 +1055,22 @@ cudaError_t launch_keys(const KeyLaunch& L, bool derive, uint32_t kpt, uint32_t 
 }
 
 cudaError_t keys_kernel(bool derive, bool incr, uint32_t kpt, uint32_t block, uint32_t layout, uint32_t dfa_smem,
-                        const void** func, size_t* dyn) {
+                        uint32_t table_smem, const void** func, size_t* dyn) {
     const bool hw = layout == LAYOUT_HASH_WARPS && !derive && !incr;
-    const void* f = hw ? hw_kernel_of(kpt, block) : kernel_of(derive, incr, kpt, block, layout == LAYOUT_ROTATING);
-    if (!f || dfa_smem > DFA_SMEM_MAX || (hw && dfa_smem)) return cudaErrorInvalidValue;
+    const uint32_t tsm = derive || incr ? 0 : table_smem;
+    const void* f = variant_kernel(derive, incr, kpt, block, layout, tsm);
+    if (!f || dfa_smem > DFA_SMEM_MAX || ((hw || tsm) && dfa_smem)) return cudaErrorInvalidValue;
     *func = f;
-    *dyn = dyn_bytes(derive, incr, block, layout) + dfa_smem;
+    *dyn = dyn_bytes(derive, incr, block, layout, tsm) + dfa_smem;
     return prepare(f, *dyn);
 }
 
-cudaError_t keys_occupancy(bool derive, bool incr, uint32_t kpt, uint32_t block, uint32_t layout, int* blocks_per_sm) {
-    const bool hw = layout == LAYOUT_HASH_WARPS && !derive && !incr;
-    const void* f = hw ? hw_kernel_of(kpt, block) : kernel_of(derive, incr, kpt, block, layout == LAYOUT_ROTATING);
+cudaError_t keys_occupancy(bool derive, bool incr, uint32_t kpt, uint32_t block, uint32_t layout, uint32_t table_smem,
+                           int* blocks_per_sm) {
+    const uint32_t tsm = derive || incr ? 0 : table_smem;
+    const void* f = variant_kernel(derive, incr, kpt, block, layout, tsm);
     if (!f) return cudaErrorInvalidValue;
-    const size_t dyn = dyn_bytes(derive, incr, block, layout);
+    const size_t dyn = dyn_bytes(derive, incr, block, layout, tsm);
     cudaError_t e = prepare(f, dyn);
     if (e != cudaSuccess) return e;
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, f, (int)block, dyn);
@@ -1091,6 +1149,97 @@ __global__ void __launch_bounds__(256) k_mad_chain_peak(uint32_t iters, uint32_t
 #pragma unroll
         for (int i = 0; i < 9; i++) s ^= acc[q][i];
     out[(uint64_t)blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+// The pieces of the field multiply's instruction mix, each on 8 independent chains per thread
+// (so latency is hidden at full occupancy and the rate is what the pipe issues):
+//   KIND 0  mad.hi.u32            the high half of a 32x32 product
+//   KIND 1  mad.wide.u32          the full 64-bit product added to a 64-bit accumulator
+//   KIND 2  madc.lo.cc.u32 rows   8 low halves linked through the carry flag (one chain per row)
+//   KIND 3  madc.hi.cc.u32 rows   8 high halves linked through the carry flag
+template <int KIND>
+__global__ void __launch_bounds__(256) k_imad_rate(uint32_t iters, uint32_t x, uint32_t y, uint32_t* out) {
+    uint32_t a[8];
+    uint64_t w[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        a[i] = threadIdx.x * 8 + i;
+        w[i] = (uint64_t)a[i] << 20;
+    }
+    for (uint32_t it = 0; it < iters; it++) {
+        if (KIND == 0) {
+#pragma unroll
+            for (int i = 0; i < 8; i++) asm volatile("mad.hi.u32 %0, %0, %1, %2;" : "+r"(a[i]) : "r"(x), "r"(y));
+        } else if (KIND == 1) {
+#pragma unroll
+            for (int i = 0; i < 8; i++) asm volatile("mad.wide.u32 %0, %1, %2, %0;" : "+l"(w[i]) : "r"(a[i]), "r"(x));
+        } else if (KIND == 2) {
+            asm volatile(
+                "mad.lo.cc.u32 %0, %8, %9, %0;\n\t"
+                "madc.lo.cc.u32 %1, %8, %9, %1;\n\t"
+                "madc.lo.cc.u32 %2, %8, %9, %2;\n\t"
+                "madc.lo.cc.u32 %3, %8, %9, %3;\n\t"
+                "madc.lo.cc.u32 %4, %8, %9, %4;\n\t"
+                "madc.lo.cc.u32 %5, %8, %9, %5;\n\t"
+                "madc.lo.cc.u32 %6, %8, %9, %6;\n\t"
+                "madc.lo.u32 %7, %8, %9, %7;\n\t"
+                : "+r"(a[0]), "+r"(a[1]), "+r"(a[2]), "+r"(a[3]), "+r"(a[4]), "+r"(a[5]), "+r"(a[6]), "+r"(a[7])
+                : "r"(x + it), "r"(y));
+        } else {
+            asm volatile(
+                "mad.hi.cc.u32 %0, %8, %9, %0;\n\t"
+                "madc.hi.cc.u32 %1, %8, %9, %1;\n\t"
+                "madc.hi.cc.u32 %2, %8, %9, %2;\n\t"
+                "madc.hi.cc.u32 %3, %8, %9, %3;\n\t"
+                "madc.hi.cc.u32 %4, %8, %9, %4;\n\t"
+                "madc.hi.cc.u32 %5, %8, %9, %5;\n\t"
+                "madc.hi.cc.u32 %6, %8, %9, %6;\n\t"
+                "madc.hi.u32 %7, %8, %9, %7;\n\t"
+                : "+r"(a[0]), "+r"(a[1]), "+r"(a[2]), "+r"(a[3]), "+r"(a[4]), "+r"(a[5]), "+r"(a[6]), "+r"(a[7])
+                : "r"(x + it), "r"(y));
+        }
+    }
+    uint32_t s = 0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) s ^= a[i] ^ (uint32_t)w[i] ^ (uint32_t)(w[i] >> 32);
+    out[(uint64_t)blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+// Rates of the four pieces (multiply-adds per second, best of three runs of 10-30 ms each).
+cudaError_t measure_imad_rates(int sms, cudaStream_t st, double rates[4]) {
+    const uint32_t blocks = (uint32_t)sms * 8, threads = 256, iters = 1u << 16;
+    uint32_t* out = nullptr;
+    cudaError_t e = cudaMalloc(&out, sizeof(uint32_t) * blocks * threads);
+    if (e != cudaSuccess) return e;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    auto launch = [&](int kind, uint32_t it, uint32_t x) {
+        if (kind == 0) k_imad_rate<0><<<blocks, threads, 0, st>>>(it, x, 0x9876u, out);
+        else if (kind == 1) k_imad_rate<1><<<blocks, threads, 0, st>>>(it, x, 0x9876u, out);
+        else if (kind == 2) k_imad_rate<2><<<blocks, threads, 0, st>>>(it, x, 0x9876u, out);
+        else k_imad_rate<3><<<blocks, threads, 0, st>>>(it, x, 0x9876u, out);
+    };
+    for (int k = 0; k < 4; k++) {
+        rates[k] = 0;
+        launch(k, iters / 16, 0x1234u);
+    }
+    for (int rep = 0; rep < 12 && e == cudaSuccess; rep++) {
+        const int k = rep % 4;
+        cudaEventRecord(e0, st);
+        launch(k, iters, 0x1234u + rep);
+        cudaEventRecord(e1, st);
+        e = cudaEventSynchronize(e1);
+        if (e == cudaSuccess) e = cudaGetLastError();
+        float ms = 0;
+        if (e == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+        const double mads = (double)blocks * threads * iters * 8;
+        if (ms > 0 && mads / (ms * 1e-3) > rates[k]) rates[k] = mads / (ms * 1e-3);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(out);
+    return e;
 }
 
 // Best of three timed runs (after a short warm-up) of both microbenchmarks, each about

@@ -37,6 +37,9 @@ struct KeyLaunch {
     // pools the products of compute threads / inv_pools threads; a divisor of the compute
     // threads, at most 32
     uint32_t inv_pools;
+    // bytes of the comb table in shared memory (search kernels; 0: gathered from HBM): every CTA
+    // copies the table there at the start, entries 96 bytes apart
+    uint32_t table_smem;
 };
 
 // LAYOUT_INVERTER_WARP: the last warp inverts, the others compute keys; LAYOUT_ROTATING: every
@@ -64,10 +67,14 @@ cudaError_t measure_field_mul_rates(int sms, cudaStream_t st, double* radix32_pe
 // The kernel of a variant and its dynamic shared memory (for graph nodes); sets the
 // kernel's shared-memory limit like launch_keys does.
 cudaError_t keys_kernel(bool derive, bool incr, uint32_t kpt, uint32_t block, uint32_t layout, uint32_t dfa_smem,
-                        const void** func, size_t* dyn);
-cudaError_t keys_occupancy(bool derive, bool incr, uint32_t kpt, uint32_t block, uint32_t layout, int* blocks_per_sm);
+                        uint32_t table_smem, const void** func, size_t* dyn);
+cudaError_t keys_occupancy(bool derive, bool incr, uint32_t kpt, uint32_t block, uint32_t layout, uint32_t table_smem,
+                           int* blocks_per_sm);
 // multiply-adds per second of the carry-chain row microbenchmark and of plain mad.lo.u32
 cudaError_t measure_mad_peaks(int sms, cudaStream_t st, double* chain_per_s, double* lo_per_s);
+// multiply-adds per second of independent mad.hi.u32, independent mad.wide.u32, and rows of
+// 8 madc.lo.cc / 8 madc.hi.cc linked through the carry flag
+cudaError_t measure_imad_rates(int sms, cudaStream_t st, double rates[4]);
 
 // Largest n of mk_derive_noalloc and the device address of its fixed staging array on the
 // current device (looked up when a context is created).

@@ -11,7 +11,7 @@ namespace mkb {
 // Rows 0..rows-2 use signed digits in [-2^(w-1), 2^(w-1)) with a carry into the next
 // row; the top row's digit is unsigned in [0, 2^w_top] and its entries include the
 // 2^254·B term.  Row i holds entries k·2^(off_i)·8B for k = 0..cols_i-1.
-constexpr int MAX_ROWS = 20;
+constexpr int MAX_ROWS = 64;  // 63 rows of 4-bit digits at most
 
 struct CombGeom {
     uint32_t rows;

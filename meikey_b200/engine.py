@@ -107,10 +107,10 @@ class Context:
 
     def __init__(self, device: int = 0, table_rows: int = 12, keys_per_thread: int = 16, block: int = 512,
                  blocks_per_sm: int = 0, self_check: bool = False, hit_capacity: int = 0, hash_warps: int = 0,
-                 inverter_rotates: bool = False, inversion_batch: int = 0):
+                 inverter_rotates: bool = False, inversion_batch: int = 0, table_in_smem: bool = False):
         self._lib = L.load()
         opts = L.Options(table_rows, keys_per_thread, block, blocks_per_sm, 1 if self_check else 0, hit_capacity,
-                         hash_warps, 1 if inverter_rotates else 0, inversion_batch)
+                         hash_warps, 1 if inverter_rotates else 0, inversion_batch, 1 if table_in_smem else 0)
         ptr = ctypes.c_void_p()
         st = self._lib.mk_ctx_create(device, ctypes.byref(opts), ctypes.byref(ptr))
         self._ptr = ptr
@@ -167,6 +167,13 @@ class Context:
         a, b = ctypes.c_double(), ctypes.c_double()
         _check(self._lib, self._ptr, self._lib.mk_measure_mad_peaks(self._ptr, ctypes.byref(a), ctypes.byref(b)))
         return a.value, b.value
+
+    def measure_imad_rates(self) -> dict:
+        """MADs/s of the field multiply's instruction pieces on independent chains (mad.hi,
+        mad.wide) and in carry-linked rows (madc.lo.cc, madc.hi.cc): mk_measure_imad_rates."""
+        v = [ctypes.c_double() for _ in range(4)]
+        _check(self._lib, self._ptr, self._lib.mk_measure_imad_rates(self._ptr, *[ctypes.byref(x) for x in v]))
+        return {"mad_hi": v[0].value, "mad_wide": v[1].value, "madc_lo_chain": v[2].value, "madc_hi_chain": v[3].value}
 
     def measure_field_mul(self):
         """(radix-2^32, radix-2^25.5, radix-2^51 FP64) field multiplications per second of the
@@ -385,7 +392,7 @@ class Graph:
 
 
 # keys/thread x block variants the library is built for
-BUILT_VARIANTS = [(4, 256), (8, 256), (16, 256), (8, 512), (16, 512)]
+BUILT_VARIANTS = [(4, 256), (8, 256), (16, 256), (4, 512), (8, 512), (16, 512)]
 
 
 def compute_threads(block: int, hash_warps: int = 0, inverter_rotates: int = 0) -> int:
@@ -403,7 +410,7 @@ def inversion_batches(keys_per_thread: int, block: int, hash_warps: int = 0, inv
 
 
 def tune_space(rows=(11, 12, 13, 14, 16), variants=BUILT_VARIANTS, blocks_per_sm=(0,), hash_warps=(0, 4),
-               inverter_rotates=(0,), inversion_batch=(0,)):
+               inverter_rotates=(0,), inversion_batch=(0,), table_in_smem=(0,)):
     """Candidate options: comb rows (table size against multiplications per key) x keys per
     thread and block x CTAs per SM x the hashing-warp layout (built for block 512, keys per
     thread 8 and 16) x who inverts (a dedicated warp, or a duty rotating over four key warps;
@@ -419,8 +426,13 @@ def tune_space(rows=(11, 12, 13, 14, 16), variants=BUILT_VARIANTS, blocks_per_sm
                             continue
                         batches = inversion_batches(k, b, h, v) if inversion_batch == "all" else inversion_batch
                         for ib in batches:
-                            out.append(dict(table_rows=r, keys_per_thread=k, block=b, blocks_per_sm=s, hash_warps=h,
-                                            inverter_rotates=v, inversion_batch=ib))
+                            for t in table_in_smem:
+                                # the shared-memory table: dedicated inverter, block 512, 4 or 8 keys
+                                if t and (h or v or b != 512 or k not in (4, 8)):
+                                    continue
+                                out.append(dict(table_rows=r, keys_per_thread=k, block=b, blocks_per_sm=s,
+                                                hash_warps=h, inverter_rotates=v, inversion_batch=ib,
+                                                table_in_smem=t))
     return out
 
 
@@ -433,7 +445,8 @@ def autotune(device: int = 0, candidates=None, finalists: int = 3, trial_keys: i
     arr = (L.TuneEntryC * len(cands))()
     for i, c in enumerate(cands):
         arr[i].options = L.Options(c["table_rows"], c["keys_per_thread"], c["block"], c.get("blocks_per_sm", 0), 1, 0,
-                                   c.get("hash_warps", 0), c.get("inverter_rotates", 0), c.get("inversion_batch", 0))
+                                   c.get("hash_warps", 0), c.get("inverter_rotates", 0), c.get("inversion_batch", 0),
+                                   c.get("table_in_smem", 0))
     best = ctypes.c_uint32()
     if job is None:
         st = lib.mk_autotune(device, arr, len(cands), finalists, trial_keys, ctypes.byref(best))
