@@ -322,6 +322,7 @@ extern "C" int mk_search_both(mk_job* job, const mk_search_config* cfg, uint32_t
     std::atomic<uint64_t> tries{0}, next_cpu{cpu_first};
     std::atomic<uint32_t> first_found{2};
     mk_outcome gpu_out{}, cpu_out{};
+    cpu_out.status = MK_ERR_STOPPED;  // no host key yet (a zeroed outcome would read as MK_OK)
     std::mutex cpu_mu;
     auto stop_all = [&] { mk_job_stop(job, 1); };
     auto claim = [&](uint32_t who) {

@@ -60,7 +60,7 @@ def test_c_program_drives_a_gpu_job(tmp_path, golden, oracle):
     for k, c in enumerate(cases):
         assert hits[k] == c["hits"], c["needle"]
         status, index, pk = int(firsts[k][0]), int(firsts[k][1]), bytes.fromhex(firsts[k][2])
-        nb = c["needle"].encode()
+        nb = c["needle"].lower().encode() if c["fold"] else c["needle"].encode()  # folded needles are lowercase
         lowest = next((i for i in c["hits"] if oracle.match(oracle.derive(key, 0, i, 1, threads=1), nb, len(nb),
                                                             c["fold"], c["mode"], False)), None)
         if lowest is not None:  # the lowest confirmed candidate of the golden range
