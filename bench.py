@@ -601,9 +601,11 @@ def measure(args, workload, steps, e2e_steps, dist, world, rank, local, cpu_seco
         inv_batch = wl.get("inversion_batch", 0)
         if inv_batch not in mk.engine.inversion_batches(kpt, args.block, hash_warps, int(rotates), 1, 1 << 20):
             inv_batch = 0
+    interleave = bool(args.hash_interleave) and source != 2
     ctx = mk.Context(device=local, table_rows=args.rows, keys_per_thread=kpt, block=args.block,
                      self_check=True, hit_capacity=(1 << 22) if workload == "multi" else 0,
-                     hash_warps=hash_warps, inverter_rotates=rotates, inversion_batch=inv_batch)
+                     hash_warps=hash_warps, inverter_rotates=rotates, inversion_batch=inv_batch,
+                     hash_interleave=interleave, table_in_smem=bool(args.table_in_smem))
     kpi = ctx.keys_per_iter
     launches = wl.get("launches", 1)  # > 1: a step is one replay of a CUDA graph of that many launches
     iters = math.ceil((args.step_candidates or wl["step"]) / (kpi * launches))
@@ -706,6 +708,8 @@ def measure(args, workload, steps, e2e_steps, dist, world, rank, local, cpu_seco
         cfg["launches_per_step"] = launches
         cfg["options_from"] = "mk_autotune sweeps of rows x keys/thread x block (profiles/autotune_sweep.md)"
         cfg["hash_warps"] = hash_warps
+        cfg["hash_interleave"] = int(interleave)
+        cfg["table_in_smem"] = int(bool(args.table_in_smem))
         cfg["inverter_rotates"] = int(rotates)
         cfg["needles"] = len(needles)
         if workload == "multi" and MULTI_SET != "all":
@@ -788,6 +792,12 @@ def main():
                     help="every warp derives keys and the inversion rotates over four warps "
                          "(mk_options.inverter_rotates; default: on for the multi-pattern workload, "
                          "the layout mk_autotune_job picks for it, off otherwise)")
+    ap.add_argument("--hash-interleave", type=int, default=0, choices=[0, 1],
+                    help="1: hash the next iteration's seeds inside the comb rows (mk_options.hash_interleave; "
+                         "ChaCha20 and counter workloads, 12 rows)")
+    ap.add_argument("--table-in-smem", action="store_true",
+                    help="every CTA keeps the comb table in shared memory (mk_options.table_in_smem; 40+ rows, "
+                         "e.g. --rows 42 --kpt 8)")
     ap.add_argument("--inversion-batch", type=int, default=None,
                     help="keys per field inversion (mk_options.inversion_batch; default: the workload's, 256 for the "
                          "secure and counter workloads where the layout can run it, else 32 pools)")

@@ -95,6 +95,12 @@ typedef struct mk_options {
                                  40+ rows, e.g. 42 rows of 6-bit digits, 133 KB; block 512, keys per thread
                                  4 or 8, the dedicated inverter; regex tables then stay in global memory).
                                  MK_ERR_OUT_OF_RANGE when the table does not fit */
+    uint32_t hash_interleave; /* 1: each thread hashes the next iteration's seeds inside the current
+                                 iteration's comb rows, 8 SHA-512 rounds per row, so that the hashing
+                                 (ALU pipe) issues between the field multiplies (IMAD pipe) of one
+                                 warp; 12 rows, block 512, keys per thread 8 or 16, the dedicated
+                                 inverter, the table in HBM.  ChaCha20 and counter seeds (the
+                                 incremental source hashes nothing) */
 } mk_options;
 
 /* One pattern as the reference's GPU needle (Needle, src/service/gpu.rs:618-660):

@@ -51,6 +51,7 @@ class Options(ctypes.Structure):
         ("inverter_rotates", ctypes.c_uint32),
         ("inversion_batch", ctypes.c_uint32),
         ("table_in_smem", ctypes.c_uint32),
+        ("hash_interleave", ctypes.c_uint32),
     ]
 
 

@@ -267,15 +267,23 @@ int mk_ctx_create(int device, const mk_options* options, mk_ctx** out) try {
     const bool smem_ok = o.table_in_smem == 0 ||
                          (o.table_in_smem == 1 && o.block == 512 && (o.keys_per_thread == 4 || o.keys_per_thread == 8) &&
                           !o.hash_warps && !o.inverter_rotates);
+    // hashing inside the comb rows: 12 rows (10 full rows carry the 80 rounds), block 512, 8 or 16
+    // keys per thread, the dedicated inverter, the table in HBM
+    const bool shai_ok = o.hash_interleave == 0 ||
+                         (o.hash_interleave == 1 && o.table_rows == 12 && o.block == 512 &&
+                          (o.keys_per_thread == 8 || o.keys_per_thread == 16) && !o.hash_warps &&
+                          !o.inverter_rotates && !o.table_in_smem);
     const bool hw_ok = o.hash_warps == 0 || (o.hash_warps == 4 && o.block == 512 && (o.keys_per_thread == 8 || o.keys_per_thread == 16));
     const bool rot_ok = o.inverter_rotates <= 1 && !(o.inverter_rotates && o.hash_warps);
-    if (o.table_rows < 10 || o.table_rows > (uint32_t)mkb::MAX_ROWS - 1 || !built || !hw_ok || !rot_ok || !smem_ok ||
+    if (o.table_rows < 10 || o.table_rows > (uint32_t)mkb::MAX_ROWS - 1 || !built || !hw_ok || !rot_ok || !smem_ok || !shai_ok ||
         o.blocks_per_sm > 16 || o.hit_capacity > (1u << 26))
         return MK_ERR_OUT_OF_RANGE;
     // inversion batch: keys per field inversion = keys per thread x compute threads / pools, with
     // the pools a divisor of the compute threads and at most 32 (one per lane of the inverting warp)
-    const uint32_t layout = o.hash_warps ? mkb::LAYOUT_HASH_WARPS : o.inverter_rotates ? mkb::LAYOUT_ROTATING
-                                                                                       : mkb::LAYOUT_INVERTER_WARP;
+    const uint32_t layout = o.hash_warps         ? mkb::LAYOUT_HASH_WARPS
+                            : o.inverter_rotates ? mkb::LAYOUT_ROTATING
+                            : o.hash_interleave  ? mkb::LAYOUT_INTERLEAVED
+                                                 : mkb::LAYOUT_INVERTER_WARP;
     const uint32_t ct = mkb::search_threads(o.block, layout);
     uint32_t pools = 32;
     if (o.inversion_batch) {

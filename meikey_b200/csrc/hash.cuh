@@ -91,6 +91,21 @@ __device__ __forceinline__ void sha512_round(u64& a, u64& b, u64& c, u64& d, u64
     h = g; g = f; f = e; e = d + t1; d = c; c = b; b = a; a = t1 + s0 + mj;
 }
 
+// The clamped scalar from the final state words a..d: digest words h0..h3 = state + IV,
+// read little-endian (the digest bytes are big-endian per word), then the RFC 8032 clamp
+// (clear bits 0-2 and 255, set bit 254).
+__device__ __forceinline__ void digest_scalar(u64 a, u64 b, u64 c, u64 d, u64 s_out[4]) {
+    u64 hh[4] = {a + MKH_IV0, b + MKH_IV1, c + MKH_IV2, d + MKH_IV3};
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        u32 hi = (u32)(hh[i] >> 32), lo = (u32)hh[i];
+        s_out[i] = (u64)bswap32(lo) << 32 | bswap32(hi);
+    }
+    s_out[0] &= ~7ull;
+    s_out[3] &= 0x7fffffffffffffffull;
+    s_out[3] |= 0x4000000000000000ull;
+}
+
 // Rounds FROM..79 of the single padded block whose message words 0..3 are `w4`
 // (words 4..15 are the fixed padding of a 32-byte message), from state `st` at the
 // start of round FROM; writes the clamped scalar as 4 little-endian u64 words
@@ -119,24 +134,19 @@ __device__ __forceinline__ void sha512_scalar_from(const u64 st[8], const u64 w4
             sha512_round(a, b, c, d, e, f, g, h, w[i], SHA512_K[blk + i]);
         }
     }
-    u64 hh[4] = {a + MKH_IV0, b + MKH_IV1, c + MKH_IV2, d + MKH_IV3};
+    digest_scalar(a, b, c, d, s_out);
+}
+
+// SHA-512 message words 0..3 (big-endian u64) of a seed given as 8 LE words
+__device__ __forceinline__ void seed_words(const u32 sw[8], u64 w4[4]) {
 #pragma unroll
-    for (int i = 0; i < 4; i++) {
-        // digest bytes are big-endian per word; the scalar reads them little-endian
-        u32 hi = (u32)(hh[i] >> 32), lo = (u32)hh[i];
-        s_out[i] = (u64)bswap32(lo) << 32 | bswap32(hi);
-    }
-    // clamp: clear bits 0-2 and 255, set bit 254
-    s_out[0] &= ~7ull;
-    s_out[3] &= 0x7fffffffffffffffull;
-    s_out[3] |= 0x4000000000000000ull;
+    for (int i = 0; i < 4; i++) w4[i] = (u64)bswap32(sw[2 * i]) << 32 | bswap32(sw[2 * i + 1]);
 }
 
 // Clamped scalar of a seed given as 8 LE words (the ChaCha20 half-block)
 __device__ __forceinline__ void seed_scalar(const u32 sw[8], u64 s_out[4]) {
     u64 w4[4];
-#pragma unroll
-    for (int i = 0; i < 4; i++) w4[i] = (u64)bswap32(sw[2 * i]) << 32 | bswap32(sw[2 * i + 1]);
+    seed_words(sw, w4);
     u64 st[8] = {MKH_IV0, MKH_IV1, MKH_IV2, MKH_IV3, MKH_IV4, MKH_IV5, MKH_IV6, MKH_IV7};
     sha512_scalar_from<0>(st, w4, s_out);
 }
@@ -162,12 +172,65 @@ __device__ __forceinline__ CounterMid counter_mid(const u32 base[8]) {
     return m;
 }
 
-__device__ __forceinline__ void counter_scalar(const CounterMid& m, u64 index, u64 s_out[4]) {
+// message words 0..3 of the counter seed of `index`
+__device__ __forceinline__ void counter_words(const CounterMid& m, u64 index, u64 w4[4]) {
     u64 tail = m.tail + index;
     // seed bytes 24..31 = LE(tail); message word 3 reads them big-endian
-    u64 w3 = (u64)bswap32((u32)tail) << 32 | bswap32((u32)(tail >> 32));
-    u64 w4[4] = {m.w[0], m.w[1], m.w[2], w3};
+    w4[0] = m.w[0];
+    w4[1] = m.w[1];
+    w4[2] = m.w[2];
+    w4[3] = (u64)bswap32((u32)tail) << 32 | bswap32((u32)(tail >> 32));
+}
+
+__device__ __forceinline__ void counter_scalar(const CounterMid& m, u64 index, u64 s_out[4]) {
+    u64 w4[4];
+    counter_words(m, index, w4);
     sha512_scalar_from<3>(m.st, w4, s_out);
+}
+
+// SHA-512 of one padded 32-byte message advanced 8 rounds at a time with the same code for
+// every step, so that a caller can interleave the steps with other work (the search kernel
+// puts one step into each comb row).  The ring w[0..15] holds W[t0-16 .. t0-1] before the step
+// of rounds t0..t0+7, t0 >= 16 (the first two steps take the message words, which start in
+// the ring); each step writes W[t0..t0+7] into w[0..7] and swaps the halves.
+struct ShaRun {
+    u64 s[8];
+    u64 w[16];
+};
+
+__device__ __forceinline__ void sha_run_start(ShaRun& r, const u64 w4[4]) {
+    r.s[0] = MKH_IV0; r.s[1] = MKH_IV1; r.s[2] = MKH_IV2; r.s[3] = MKH_IV3;
+    r.s[4] = MKH_IV4; r.s[5] = MKH_IV5; r.s[6] = MKH_IV6; r.s[7] = MKH_IV7;
+#pragma unroll
+    for (int i = 0; i < 4; i++) r.w[i] = w4[i];
+    r.w[4] = 0x8000000000000000ull;
+#pragma unroll
+    for (int i = 5; i < 15; i++) r.w[i] = 0;
+    r.w[15] = 256;
+}
+
+// rounds t0..t0+7 (t0 = 0, 8, ..., 72)
+__device__ __forceinline__ void sha_run_step(ShaRun& r, u32 t0) {
+    const bool sched = t0 >= 16;
+    u64 a = r.s[0], b = r.s[1], c = r.s[2], d = r.s[3], e = r.s[4], f = r.s[5], g = r.s[6], h = r.s[7];
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        const u64 x2 = i < 2 ? r.w[i + 14] : r.w[i - 2];   // W[t-2]
+        const u64 x7 = i < 7 ? r.w[i + 9] : r.w[0];        // W[t-7]
+        const u64 x15 = r.w[i + 1];                         // W[t-15]
+        const u64 s0 = rotr64(x15, 1) ^ rotr64(x15, 8) ^ (x15 >> 7);
+        const u64 s1 = rotr64(x2, 19) ^ rotr64(x2, 61) ^ (x2 >> 6);
+        const u64 wt = sched ? r.w[i] + s0 + x7 + s1 : r.w[i];
+        r.w[i] = wt;
+        sha512_round(a, b, c, d, e, f, g, h, wt, SHA512_K[t0 + i]);
+    }
+    r.s[0] = a; r.s[1] = b; r.s[2] = c; r.s[3] = d; r.s[4] = e; r.s[5] = f; r.s[6] = g; r.s[7] = h;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        const u64 t = r.w[i];
+        r.w[i] = r.w[i + 8];
+        r.w[i + 8] = t;
+    }
 }
 
 }  // namespace mkh

@@ -208,6 +208,44 @@ __device__ __forceinline__ void comb_mul(const uint4* __restrict__ table, const 
     mk32::ge_add_niels_frac(P, n, yn, yd, xn, xd);
 }
 
+// comb_mul with one 8-round step of the SHA-512 `run` (the next iteration's seed) in every
+// full-addition row, in the same straight-line block as the row's field multiplies, so that
+// the hashing (ALU pipe) issues between the multiplies (IMAD pipe).  Built for 12 rows: the
+// 10 full rows carry the 80 rounds.  y = yn/yd only.
+__device__ __forceinline__ void comb_mul_sha(const uint4* __restrict__ table, const CombGeom& g, const u64 s[4],
+                                             EntrySlot& slot, fe& yn, fe& yd, mkh::ShaRun& run) {
+    u64 m[4];
+    comb_m(s, m);
+    const u32 rows = g.rows;
+    int carry = 0;
+    int d0 = next_digit(g, m, 0, carry);
+    fetch_entry(slot, 0, table, entry_index(g, 0, d0));
+    int dn = next_digit(g, m, 1, carry);
+    fetch_entry(slot, 1, table, entry_index(g, 1, dn));
+    wait_entries<1>();
+    ge P = comb_row0(read_entry(slot, 0), d0 < 0);
+#pragma unroll 1
+    for (u32 row = 1; row + 1 < rows; row++) {
+        const int d = dn;
+        // the next row's digit without a branch (the top row's is unsigned: the carry lands
+        // in it unchanged)
+        int c2 = carry;
+        const int sd = next_digit(g, m, row + 1, c2);
+        const int td = (int)bits_at(m, g.offset[row + 1], g.width[row + 1]) + carry;
+        const bool top = row + 2 >= rows;
+        dn = top ? td : sd;
+        carry = top ? carry : c2;
+        fetch_entry(slot, (row + 1) & 1, table, entry_index(g, row + 1, dn));
+        wait_entries<1>();
+        niels n = read_entry(slot, row & 1);
+        mkh::sha_run_step(run, 8u * (row - 1));
+        P = mk32::ge_add_niels(P, n, d < 0);
+    }
+    wait_entries<0>();
+    niels n = read_entry(slot, (rows - 1) & 1);
+    mk32::ge_add_niels_frac(P, n, yn, yd, nullptr, nullptr);
+}
+
 // 6-bit values of the 44-character base64 tail of the key blob (0x20 then the key),
 // from the key's 8 little-endian words; only positions 1..43 are searched.
 __device__ __forceinline__ u32 tail_value(const u32 pk[8], int pos) {
@@ -438,6 +476,57 @@ __device__ __forceinline__ void combs(const KeyLaunch& L, const CombGeom& g, con
     b.prod = run;
 }
 
+// Comb multiplies of this iteration's KPT scalars (sc) with the SHA-512 of the next
+// iteration's seeds (indices next_first + j) carried through their rows: key j's comb reads
+// sc[j] at its start and leaves the next iteration's scalar of key j there.  ChaCha20 blocks
+// serve an even index and the next odd one (the other half is kept).
+template <int KPT>
+__device__ __forceinline__ void combs_sha(const KeyLaunch& L, const CombGeom& g, u64 sc[KPT][4], EntrySlot& slot,
+                                          Batch<KPT>& b, const u32 key[8], const mkh::CounterMid& mid,
+                                          u64 next_first) {
+    fe run;
+    u32 other[8];
+    u64 other_id = ~0ull;
+#pragma unroll 1
+    for (int j = 0; j < KPT; j++) {
+        const u64 idx = next_first + (u64)j;
+        u64 w4[4];
+        if (L.seed_src == 1) {
+            mkh::counter_words(mid, idx, w4);
+        } else {
+            u32 sw[8];
+            if ((idx >> 1) == other_id) {
+#pragma unroll
+                for (int i = 0; i < 8; i++) sw[i] = other[i];
+            } else {
+                u32 blk[16];
+                mkh::chacha20_block(key, idx >> 1, blk);
+                const bool odd = idx & 1;
+#pragma unroll
+                for (int i = 0; i < 8; i++) {
+                    sw[i] = odd ? blk[8 + i] : blk[i];
+                    other[i] = odd ? blk[i] : blk[8 + i];
+                }
+                other_id = idx >> 1;
+            }
+            mkh::seed_words(sw, w4);
+        }
+        mkh::ShaRun shr;
+        mkh::sha_run_start(shr, w4);
+        fe num;
+        comb_mul_sha(L.table, g, sc[j], slot, num, b.den[j], shr);
+        mkh::digest_scalar(shr.s[0], shr.s[1], shr.s[2], shr.s[3], sc[j]);
+        if (j == 0) {
+            b.a[0] = num;
+            run = b.den[0];
+        } else {
+            b.a[j] = mk32::fe_mul(num, run);
+            run = mk32::fe_mul(run, b.den[j]);
+        }
+    }
+    b.prod = run;
+}
+
 // Backward pass: `inv` is 1/(product of the batch's denominators); yields each key's
 // canonical y (sign bit 0), tests the needles and reports candidate hits.
 template <int KPT>
@@ -586,7 +675,9 @@ __device__ __forceinline__ void incr_fracs(const ge& Q, const uint4* steps, Batc
 // keys_per_iter·B (one mixed addition) per iteration.  No comb table is read.
 // STAB: the comb table lives in shared memory (copied by every CTA at the start, in place of
 // the staging slots; tables of a few hundred to a few thousand entries, 40+ rows).
-template <int KPT, int BLOCK, bool INCR, bool ROT, bool STAB = false>
+// SHAI: the SHA-512 of iteration it+1's seeds runs inside iteration it's comb rows (12 rows;
+// the first iteration's scalars are hashed up front).
+template <int KPT, int BLOCK, bool INCR, bool ROT, bool STAB = false, bool SHAI = false>
 __global__ void __launch_bounds__(BLOCK, 512 / BLOCK) k_search(const KeyLaunch L) {
     constexpr int CT = ROT ? BLOCK : BLOCK - 32;  // compute threads
     constexpr int CW = CT / 32;                   // compute warps
@@ -691,6 +782,9 @@ __global__ void __launch_bounds__(BLOCK, 512 / BLOCK) k_search(const KeyLaunch L
         if (INCR) {
             incr_fracs<KPT>(Q, steps, batch[b]);
             Q = mk32::ge_add_niels(Q, words_niels(L.delta), false);
+        } else if (SHAI) {
+            if (it == 0) scalars<KPT>(L, key, mid, first_of(0), sc);
+            combs_sha<KPT>(L, g, sc, slot, batch[b], key, mid, first_of(it + 1));
         } else {
             scalars<KPT>(L, key, mid, first_of(it), sc);
             combs<KPT, STAB>(L, g, sc, slot, stab, batch[b]);
@@ -993,6 +1087,7 @@ static size_t dyn_bytes(bool derive, bool incr, uint32_t block, uint32_t layout,
         return 4 * ct * fe_bytes + ct * sizeof(EntrySlot) + 2 * 4 * ct * 32;
     }
     const size_t threads = derive ? block : search_threads(block, layout == LAYOUT_HASH_WARPS ? LAYOUT_INVERTER_WARP : layout);
+    // (the interleaved layout has the dedicated inverter's buffers)
     if (table_smem && !derive && !incr) return 4 * threads * fe_bytes + table_smem;  // the table in place of the slots
     return (derive ? 2 : 4) * threads * fe_bytes + (incr ? 0 : threads * sizeof(EntrySlot));
 }
@@ -1029,9 +1124,19 @@ static cudaError_t prepare(const void* f, size_t dyn) {
     return cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
 }
 
+// search kernels with the SHA-512 interleaved into the comb rows: the dedicated-inverter layout,
+// block 512, keys per thread 8 and 16
+static const void* shai_kernel_of(uint32_t kpt, uint32_t block) {
+    if (block != 512) return nullptr;
+    if (kpt == 8) return (const void*)k_search<8, 512, false, false, false, true>;
+    if (kpt == 16) return (const void*)k_search<16, 512, false, false, false, true>;
+    return nullptr;
+}
+
 // the kernel of a variant (the table-in-shared-memory search when table_smem > 0)
 static const void* variant_kernel(bool derive, bool incr, uint32_t kpt, uint32_t block, uint32_t layout,
                                   uint32_t table_smem) {
+    if (layout == LAYOUT_INTERLEAVED && !derive && !incr) return table_smem ? nullptr : shai_kernel_of(kpt, block);
     const bool hw = layout == LAYOUT_HASH_WARPS && !derive && !incr;
     if (table_smem && !derive && !incr) return layout == LAYOUT_INVERTER_WARP ? stab_kernel_of(kpt, block) : nullptr;
     return hw ? hw_kernel_of(kpt, block) : kernel_of(derive, incr, kpt, block, layout == LAYOUT_ROTATING);

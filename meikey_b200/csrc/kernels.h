@@ -43,9 +43,11 @@ struct KeyLaunch {
 };
 
 // LAYOUT_INVERTER_WARP: the last warp inverts, the others compute keys; LAYOUT_ROTATING: every
-// warp computes keys and the inversion rotates over four warps; LAYOUT_HASH_WARPS: 11 comb
-// warps, 1 inverter, 4 hashing warps (k_search_hw; ChaCha20 / counter seeds)
-constexpr uint32_t LAYOUT_INVERTER_WARP = 0, LAYOUT_ROTATING = 1, LAYOUT_HASH_WARPS = 4;
+// warp computes keys and the inversion rotates over four warps; LAYOUT_INTERLEAVED: as
+// LAYOUT_INVERTER_WARP, with each iteration's SHA-512 of the next iteration's seeds inside the
+// comb rows (12 rows); LAYOUT_HASH_WARPS: 11 comb warps, 1 inverter, 4 hashing warps
+// (k_search_hw; ChaCha20 / counter seeds)
+constexpr uint32_t LAYOUT_INVERTER_WARP = 0, LAYOUT_ROTATING = 1, LAYOUT_INTERLEAVED = 2, LAYOUT_HASH_WARPS = 4;
 
 // compute threads of a search CTA
 inline uint32_t search_threads(uint32_t block, uint32_t layout) {

@@ -107,10 +107,12 @@ class Context:
 
     def __init__(self, device: int = 0, table_rows: int = 12, keys_per_thread: int = 16, block: int = 512,
                  blocks_per_sm: int = 0, self_check: bool = False, hit_capacity: int = 0, hash_warps: int = 0,
-                 inverter_rotates: bool = False, inversion_batch: int = 0, table_in_smem: bool = False):
+                 inverter_rotates: bool = False, inversion_batch: int = 0, table_in_smem: bool = False,
+                 hash_interleave: bool = False):
         self._lib = L.load()
         opts = L.Options(table_rows, keys_per_thread, block, blocks_per_sm, 1 if self_check else 0, hit_capacity,
-                         hash_warps, 1 if inverter_rotates else 0, inversion_batch, 1 if table_in_smem else 0)
+                         hash_warps, 1 if inverter_rotates else 0, inversion_batch, 1 if table_in_smem else 0,
+                         1 if hash_interleave else 0)
         ptr = ctypes.c_void_p()
         st = self._lib.mk_ctx_create(device, ctypes.byref(opts), ctypes.byref(ptr))
         self._ptr = ptr
@@ -446,7 +448,7 @@ def autotune(device: int = 0, candidates=None, finalists: int = 3, trial_keys: i
     for i, c in enumerate(cands):
         arr[i].options = L.Options(c["table_rows"], c["keys_per_thread"], c["block"], c.get("blocks_per_sm", 0), 1, 0,
                                    c.get("hash_warps", 0), c.get("inverter_rotates", 0), c.get("inversion_batch", 0),
-                                   c.get("table_in_smem", 0))
+                                   c.get("table_in_smem", 0), c.get("hash_interleave", 0))
     best = ctypes.c_uint32()
     if job is None:
         st = lib.mk_autotune(device, arr, len(cands), finalists, trial_keys, ctypes.byref(best))
