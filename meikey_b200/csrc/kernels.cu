@@ -1256,57 +1256,64 @@ __global__ void __launch_bounds__(256) k_mad_chain_peak(uint32_t iters, uint32_t
     out[(uint64_t)blockIdx.x * blockDim.x + threadIdx.x] = s;
 }
 
-// The pieces of the field multiply's instruction mix, each on 8 independent chains per thread
-// (so latency is hidden at full occupancy and the rate is what the pipe issues):
-//   KIND 0  mad.hi.u32            the high half of a 32x32 product
-//   KIND 1  mad.wide.u32          the full 64-bit product added to a 64-bit accumulator
-//   KIND 2  madc.lo.cc.u32 rows   8 low halves linked through the carry flag (one chain per row)
-//   KIND 3  madc.hi.cc.u32 rows   8 high halves linked through the carry flag
+// The pieces of the field multiply's instruction mix, each on 8 chains per thread (so latency
+// is hidden at full occupancy and the rate is what the pipe issues).  Every product has an
+// operand that changes every iteration and differs between the chains, so no product can be
+// hoisted out of the loop or shared between chains:
+//   KIND 0  mad.hi.u32            the high half of a 32x32 product (independent chains)
+//   KIND 1  mad.wide.u32          the full 64-bit product into a 64-bit sum (independent chains)
+//   KIND 2  madc.lo.cc.u32 rows   8 low halves a_i·b linked through the carry flag
+//   KIND 3  madc.hi.cc.u32 rows   8 high halves a_i·b linked through the carry flag
 template <int KIND>
 __global__ void __launch_bounds__(256) k_imad_rate(uint32_t iters, uint32_t x, uint32_t y, uint32_t* out) {
-    uint32_t a[8];
+    uint32_t a[8], t[8];
     uint64_t w[8];
 #pragma unroll
     for (int i = 0; i < 8; i++) {
-        a[i] = threadIdx.x * 8 + i;
+        a[i] = (threadIdx.x * 8 + i) * 0x9e3779b9u + x;
+        t[i] = threadIdx.x ^ (i * 0x01010101u);
         w[i] = (uint64_t)a[i] << 20;
     }
     for (uint32_t it = 0; it < iters; it++) {
         if (KIND == 0) {
 #pragma unroll
-            for (int i = 0; i < 8; i++) asm volatile("mad.hi.u32 %0, %0, %1, %2;" : "+r"(a[i]) : "r"(x), "r"(y));
+            for (int i = 0; i < 8; i++) asm volatile("mad.hi.u32 %0, %0, %1, %2;" : "+r"(t[i]) : "r"(a[i]), "r"(y));
         } else if (KIND == 1) {
 #pragma unroll
-            for (int i = 0; i < 8; i++) asm volatile("mad.wide.u32 %0, %1, %2, %0;" : "+l"(w[i]) : "r"(a[i]), "r"(x));
-        } else if (KIND == 2) {
-            asm volatile(
-                "mad.lo.cc.u32 %0, %8, %9, %0;\n\t"
-                "madc.lo.cc.u32 %1, %8, %9, %1;\n\t"
-                "madc.lo.cc.u32 %2, %8, %9, %2;\n\t"
-                "madc.lo.cc.u32 %3, %8, %9, %3;\n\t"
-                "madc.lo.cc.u32 %4, %8, %9, %4;\n\t"
-                "madc.lo.cc.u32 %5, %8, %9, %5;\n\t"
-                "madc.lo.cc.u32 %6, %8, %9, %6;\n\t"
-                "madc.lo.u32 %7, %8, %9, %7;\n\t"
-                : "+r"(a[0]), "+r"(a[1]), "+r"(a[2]), "+r"(a[3]), "+r"(a[4]), "+r"(a[5]), "+r"(a[6]), "+r"(a[7])
-                : "r"(x + it), "r"(y));
+            for (int i = 0; i < 8; i++)  // the multiplier is the sum's own low word
+                asm volatile("{\n\t.reg .u32 m;\n\tcvt.u32.u64 m, %0;\n\tmad.wide.u32 %0, m, %1, %0;\n\t}"
+                             : "+l"(w[i]) : "r"(a[i]));
         } else {
-            asm volatile(
-                "mad.hi.cc.u32 %0, %8, %9, %0;\n\t"
-                "madc.hi.cc.u32 %1, %8, %9, %1;\n\t"
-                "madc.hi.cc.u32 %2, %8, %9, %2;\n\t"
-                "madc.hi.cc.u32 %3, %8, %9, %3;\n\t"
-                "madc.hi.cc.u32 %4, %8, %9, %4;\n\t"
-                "madc.hi.cc.u32 %5, %8, %9, %5;\n\t"
-                "madc.hi.cc.u32 %6, %8, %9, %6;\n\t"
-                "madc.hi.u32 %7, %8, %9, %7;\n\t"
-                : "+r"(a[0]), "+r"(a[1]), "+r"(a[2]), "+r"(a[3]), "+r"(a[4]), "+r"(a[5]), "+r"(a[6]), "+r"(a[7])
-                : "r"(x + it), "r"(y));
+            const uint32_t b = t[7] + it;
+            if (KIND == 2)
+                asm volatile(
+                    "mad.lo.cc.u32 %0, %8, %16, %0;\n\t"
+                    "madc.lo.cc.u32 %1, %9, %16, %1;\n\t"
+                    "madc.lo.cc.u32 %2, %10, %16, %2;\n\t"
+                    "madc.lo.cc.u32 %3, %11, %16, %3;\n\t"
+                    "madc.lo.cc.u32 %4, %12, %16, %4;\n\t"
+                    "madc.lo.cc.u32 %5, %13, %16, %5;\n\t"
+                    "madc.lo.cc.u32 %6, %14, %16, %6;\n\t"
+                    "madc.lo.u32 %7, %15, %16, %7;\n\t"
+                    : "+r"(t[0]), "+r"(t[1]), "+r"(t[2]), "+r"(t[3]), "+r"(t[4]), "+r"(t[5]), "+r"(t[6]), "+r"(t[7])
+                    : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(a[4]), "r"(a[5]), "r"(a[6]), "r"(a[7]), "r"(b));
+            else
+                asm volatile(
+                    "mad.hi.cc.u32 %0, %8, %16, %0;\n\t"
+                    "madc.hi.cc.u32 %1, %9, %16, %1;\n\t"
+                    "madc.hi.cc.u32 %2, %10, %16, %2;\n\t"
+                    "madc.hi.cc.u32 %3, %11, %16, %3;\n\t"
+                    "madc.hi.cc.u32 %4, %12, %16, %4;\n\t"
+                    "madc.hi.cc.u32 %5, %13, %16, %5;\n\t"
+                    "madc.hi.cc.u32 %6, %14, %16, %6;\n\t"
+                    "madc.hi.u32 %7, %15, %16, %7;\n\t"
+                    : "+r"(t[0]), "+r"(t[1]), "+r"(t[2]), "+r"(t[3]), "+r"(t[4]), "+r"(t[5]), "+r"(t[6]), "+r"(t[7])
+                    : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(a[4]), "r"(a[5]), "r"(a[6]), "r"(a[7]), "r"(b));
         }
     }
     uint32_t s = 0;
 #pragma unroll
-    for (int i = 0; i < 8; i++) s ^= a[i] ^ (uint32_t)w[i] ^ (uint32_t)(w[i] >> 32);
+    for (int i = 0; i < 8; i++) s ^= t[i] ^ (uint32_t)w[i] ^ (uint32_t)(w[i] >> 32);
     out[(uint64_t)blockIdx.x * blockDim.x + threadIdx.x] = s;
 }
 
