@@ -763,6 +763,51 @@ def run_ours(args):
     return 0
 
 
+def tune_candidates(workload):
+    """The tuning space the multi-pattern configuration names, in three groups around the
+    default point (12 rows, 8 keys per thread, block 512): comb windows (rows 10-20 from HBM,
+    32 rows = 8-bit digits from HBM, 42 / 45 / 63 rows = 6-, 5-, 4-bit digits from shared
+    memory), keys per thread x block x who inverts, and the inversion batch (64-512)."""
+    from meikey_b200.engine import inversion_batches
+    rot = int(WORKLOADS[workload].get("inverter_rotates", False))
+    base = dict(table_rows=12, keys_per_thread=8, block=512, inverter_rotates=rot)
+    out = []
+    for rows in (10, 11, 12, 13, 14, 16, 20, 32):
+        out.append(dict(base, table_rows=rows))
+    for rows, kpt in ((42, 8), (45, 8), (63, 8), (42, 4)):
+        out.append(dict(base, table_rows=rows, keys_per_thread=kpt, inverter_rotates=0, table_in_smem=1))
+    for kpt, block in ((4, 256), (8, 256), (16, 256), (4, 512), (16, 512)):
+        for r in (0, 1):
+            out.append(dict(base, keys_per_thread=kpt, block=block, inverter_rotates=r))
+    for kpt in (8, 16):
+        for r in (0, 1):
+            for ib in inversion_batches(kpt, 512, 0, r, 64, 512):
+                out.append(dict(base, keys_per_thread=kpt, inverter_rotates=r, inversion_batch=ib))
+    out.append(dict(base, inverter_rotates=0, hash_interleave=1))
+    out.append(dict(base, inverter_rotates=0, hash_warps=4))
+    return out
+
+
+def run_autotune(args):
+    """mk_autotune_job over tune_candidates() on the workload's own job; one JSON line per
+    candidate, then the pick."""
+    import meikey_b200 as mk
+    from meikey_b200.engine import autotune
+    wl = WORKLOADS[args.workload]
+    cands = tune_candidates(args.workload)
+    # the field radix: the search kernel is built for radix 2^32; the others are timed here
+    with mk.Context(device=0, table_rows=16, keys_per_thread=8) as c:
+        r32, r26, r51 = c.measure_field_mul()
+    best, results = autotune(0, cands, finalists=4, trial_keys=args.tune_keys,
+                             job=(workload_key(args.workload), wl["source"], workload_needles(args.workload)))
+    for r in results:
+        print(json.dumps(r), flush=True)
+    print(json.dumps({"workload": args.workload, "best": best, "candidates": len(cands),
+                      "field_mul_per_s": {"radix_2^32": r32, "radix_2^25.5": r26, "radix_2^51_fp64": r51}}),
+          flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__)
     ap.add_argument("--gpus", type=int, default=1)
@@ -795,6 +840,10 @@ def main():
     ap.add_argument("--hash-interleave", type=int, default=0, choices=[0, 1],
                     help="1: hash the next iteration's seeds inside the comb rows (mk_options.hash_interleave; "
                          "ChaCha20 and counter workloads, 12 rows)")
+    ap.add_argument("--autotune", action="store_true",
+                    help="instead of the benchmark: mk_autotune_job over the tuning space on the workload's job "
+                         "(comb windows, keys per thread, layouts, inversion batches); prints every candidate")
+    ap.add_argument("--tune-keys", type=int, default=1 << 27, help="autotune: candidates per trial launch")
     ap.add_argument("--table-in-smem", action="store_true",
                     help="every CTA keeps the comb table in shared memory (mk_options.table_in_smem; 40+ rows, "
                          "e.g. --rows 42 --kpt 8)")
@@ -809,6 +858,8 @@ def main():
     args = ap.parse_args()
     global MULTI_SET
     MULTI_SET = args.multi_set
+    if args.autotune:
+        return run_autotune(args)
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "serving":
