@@ -50,10 +50,10 @@ WORKLOADS = {
     # the reference's published GPU mode (docs/benchmark.md): low-security counter seeds, the
     # needle TARGET case-insensitive
     "counter": {"total": 1 << 33, "step": 1 << 30, "source": 1, "seed": 7, "length": 0, "mode": "contains_ci",
-                "needle": "TARGET", "inversion_batch": 256},
+                "needle": "TARGET", "kpt": 4},
     "incremental": {"total": 1 << 32, "step": 1 << 28, "source": 2, "seed": 11, "length": 6, "mode": "suffix"},
     "multi": {"total": 1 << 34, "step": 1 << 30, "source": 0, "seed": 23, "length": 0, "mode": "mixed",
-              "launches": 4, "inverter_rotates": True},
+              "launches": 4, "inverter_rotates": True, "kpt": 16, "inversion_batch": 256},
     "serving": {"total": 0, "step": 0, "source": 0, "seed": 31, "length": 0, "mode": "mixed", "jobs": 1000,
                 "rate": 50.0, "budget": 1 << 26, "iters_per_tick": 8, "device_bytes": 32 << 20},
 }
@@ -592,7 +592,9 @@ def measure(args, workload, steps, e2e_steps, dist, world, rank, local, cpu_seco
     wl = WORKLOADS[workload]
     key, source = workload_key(workload), wl["source"]
     # the multi-pattern workload's 3-character patterns alone give ~1e-3 candidates per key
-    kpt = args.kpt or (16 if source == 2 else 8)
+    # keys per thread: the workload's (the tuner's pick, profiles/autotune_sweep.md), else 16 for
+    # the incremental source and 8 for the hashed ones
+    kpt = args.kpt or wl.get("kpt") or (16 if source == 2 else 8)
     rotates = args.inverter_rotates if args.inverter_rotates is not None else bool(wl.get("inverter_rotates", False))
     hash_warps = args.hash_warps if source != 2 else 0
     inv_batch = args.inversion_batch
@@ -706,7 +708,8 @@ def measure(args, workload, steps, e2e_steps, dist, world, rank, local, cpu_seco
         }
         cfg = workload_config(workload, ctx, step_keys, steps)
         cfg["launches_per_step"] = launches
-        cfg["options_from"] = "mk_autotune sweeps of rows x keys/thread x block (profiles/autotune_sweep.md)"
+        cfg["options_from"] = ("mk_autotune_job sweeps (profiles/autotune_sweep.md); the secure headline keeps 8 keys "
+                               "per thread, the layout that forms the configuration's inversion batch of 256")
         cfg["hash_warps"] = hash_warps
         cfg["hash_interleave"] = int(interleave)
         cfg["table_in_smem"] = int(bool(args.table_in_smem))
