@@ -173,14 +173,144 @@ __device__ __forceinline__ fe fe_reduce512(const u32 t[16]) {
           "+r"(t[I + 6]), "+r"(t[I + 7]), "+r"(t[I + 8])                                            \
         : "r"(a.v[1]), "r"(a.v[3]), "r"(a.v[5]), "r"(a.v[7]), "r"(b.v[I]));
 
-// r = a·b mod p (as a value below 2^256)
-__device__ __forceinline__ fe fe_mul(const fe& a, const fe& b) {
+// r = a·b mod p (as a value below 2^256), schoolbook: 64 lo + 64 hi products
+__device__ __forceinline__ fe fe_mul_schoolbook(const fe& a, const fe& b) {
     u32 t[16];
 #pragma unroll
     for (int i = 0; i < 16; i++) t[i] = 0;
     // after row I the partial sum is below 2^(32(I+9)), so word I+8 absorbs the final carry
     MK32_ROW(0) MK32_ROW(1) MK32_ROW(2) MK32_ROW(3) MK32_ROW(4) MK32_ROW(5) MK32_ROW(6) MK32_ROW(7)
     return fe_reduce512(t);
+}
+
+// One row of a 128 x 128-bit product: T[I..I+4] += X · Y_I, the even X limbs in one carry
+// chain and the odd ones in a second; after row I the sum is below 2^(32(I+5)).
+#define MK32_ROW4(T, X, Y, I)                                                                        \
+    asm("mad.lo.cc.u32 %0, %5, %7, %0;\n\t"                                                          \
+        "madc.hi.cc.u32 %1, %5, %7, %1;\n\t"                                                         \
+        "madc.lo.cc.u32 %2, %6, %7, %2;\n\t"                                                         \
+        "madc.hi.cc.u32 %3, %6, %7, %3;\n\t"                                                         \
+        "addc.u32 %4, %4, 0;\n\t"                                                                    \
+        : "+r"(T[I]), "+r"(T[I + 1]), "+r"(T[I + 2]), "+r"(T[I + 3]), "+r"(T[I + 4])                 \
+        : "r"(X[0]), "r"(X[2]), "r"(Y[I]));                                                          \
+    asm("mad.lo.cc.u32 %0, %4, %6, %0;\n\t"                                                          \
+        "madc.hi.cc.u32 %1, %4, %6, %1;\n\t"                                                         \
+        "madc.lo.cc.u32 %2, %5, %6, %2;\n\t"                                                         \
+        "madc.hi.u32 %3, %5, %6, %3;\n\t"                                                            \
+        : "+r"(T[I + 1]), "+r"(T[I + 2]), "+r"(T[I + 3]), "+r"(T[I + 4])                             \
+        : "r"(X[1]), "r"(X[3]), "r"(Y[I]));
+
+// t[0..7] = x · y for 128-bit x, y (four limbs each): 16 lo + 16 hi products
+__device__ __forceinline__ void mul128(const u32 x[4], const u32 y[4], u32 t[8]) {
+#pragma unroll
+    for (int i = 0; i < 8; i++) t[i] = 0;
+    MK32_ROW4(t, x, y, 0) MK32_ROW4(t, x, y, 1) MK32_ROW4(t, x, y, 2) MK32_ROW4(t, x, y, 3)
+}
+
+// d = |x - y| for 128-bit x, y; returns all ones when x < y, else 0
+__device__ __forceinline__ u32 absdiff128(const u32 x[4], const u32 y[4], u32 d[4]) {
+    u32 s;
+    asm("sub.cc.u32 %0, %5, %9;\n\t"
+        "subc.cc.u32 %1, %6, %10;\n\t"
+        "subc.cc.u32 %2, %7, %11;\n\t"
+        "subc.cc.u32 %3, %8, %12;\n\t"
+        "subc.u32 %4, 0, 0;\n\t"
+        : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3]), "=r"(s)
+        : "r"(x[0]), "r"(x[1]), "r"(x[2]), "r"(x[3]), "r"(y[0]), "r"(y[1]), "r"(y[2]), "r"(y[3]));
+    // negative: (d ^ s) - s = 2^128 - d, the magnitude
+#pragma unroll
+    for (int i = 0; i < 4; i++) d[i] ^= s;
+    asm("sub.cc.u32 %0, %0, %4;\n\t"
+        "subc.cc.u32 %1, %1, %4;\n\t"
+        "subc.cc.u32 %2, %2, %4;\n\t"
+        "subc.u32 %3, %3, %4;\n\t"
+        : "+r"(d[0]), "+r"(d[1]), "+r"(d[2]), "+r"(d[3])
+        : "r"(s));
+    return s;
+}
+
+// r = a·b mod p by one level of subtractive Karatsuba on the 128-bit halves
+// (a = A1·2^128 + A0): A0·B1 + A1·B0 = L + H ± |A0 - A1|·|B1 - B0| with L = A0·B0 and
+// H = A1·B1, so the 512-bit product takes 48 lo + 48 hi products and about 60 adds and
+// logic operations instead of 64 + 64.  The product t is the same 512-bit integer as the
+// schoolbook's, and so is the folded result.
+__device__ __forceinline__ fe fe_mul_karatsuba(const fe& a, const fe& b) {
+    u32 da[4], db[4], mm[8], lo[8], hi[8], mid[9];
+    const u32 sa = absdiff128(&a.v[0], &a.v[4], da);
+    const u32 sb = absdiff128(&b.v[4], &b.v[0], db);
+    const u32 s = sa ^ sb;  // all ones: the middle product is subtracted
+    mul128(da, db, mm);
+    mul128(&a.v[0], &b.v[0], lo);
+    mul128(&a.v[4], &b.v[4], hi);
+    // mid = L + H, nine words
+    asm("add.cc.u32 %0, %9, %17;\n\t"
+        "addc.cc.u32 %1, %10, %18;\n\t"
+        "addc.cc.u32 %2, %11, %19;\n\t"
+        "addc.cc.u32 %3, %12, %20;\n\t"
+        "addc.cc.u32 %4, %13, %21;\n\t"
+        "addc.cc.u32 %5, %14, %22;\n\t"
+        "addc.cc.u32 %6, %15, %23;\n\t"
+        "addc.cc.u32 %7, %16, %24;\n\t"
+        "addc.u32 %8, 0, 0;\n\t"
+        : "=r"(mid[0]), "=r"(mid[1]), "=r"(mid[2]), "=r"(mid[3]), "=r"(mid[4]), "=r"(mid[5]), "=r"(mid[6]),
+          "=r"(mid[7]), "=r"(mid[8])
+        : "r"(lo[0]), "r"(lo[1]), "r"(lo[2]), "r"(lo[3]), "r"(lo[4]), "r"(lo[5]), "r"(lo[6]), "r"(lo[7]),
+          "r"(hi[0]), "r"(hi[1]), "r"(hi[2]), "r"(hi[3]), "r"(hi[4]), "r"(hi[5]), "r"(hi[6]), "r"(hi[7]));
+    // mid += ±M mod 2^288: (M ^ s) with a ninth word s, plus a carry-in of s & 1 (set by s + s);
+    // the true value A0·B1 + A1·B0 lies in [0, 2^257)
+#pragma unroll
+    for (int i = 0; i < 8; i++) mm[i] ^= s;
+    u32 scratch;
+    asm("add.cc.u32 %9, %10, %10;\n\t"
+        "addc.cc.u32 %0, %0, %11;\n\t"
+        "addc.cc.u32 %1, %1, %12;\n\t"
+        "addc.cc.u32 %2, %2, %13;\n\t"
+        "addc.cc.u32 %3, %3, %14;\n\t"
+        "addc.cc.u32 %4, %4, %15;\n\t"
+        "addc.cc.u32 %5, %5, %16;\n\t"
+        "addc.cc.u32 %6, %6, %17;\n\t"
+        "addc.cc.u32 %7, %7, %18;\n\t"
+        "addc.u32 %8, %8, %10;\n\t"
+        : "+r"(mid[0]), "+r"(mid[1]), "+r"(mid[2]), "+r"(mid[3]), "+r"(mid[4]), "+r"(mid[5]), "+r"(mid[6]),
+          "+r"(mid[7]), "+r"(mid[8]), "=r"(scratch)
+        : "r"(s), "r"(mm[0]), "r"(mm[1]), "r"(mm[2]), "r"(mm[3]), "r"(mm[4]), "r"(mm[5]), "r"(mm[6]), "r"(mm[7]));
+    // t = L + mid·2^128 + H·2^256 (below 2^512: no carry out of word 15)
+    u32 t[16];
+    t[0] = lo[0];
+    t[1] = lo[1];
+    t[2] = lo[2];
+    t[3] = lo[3];
+    asm("add.cc.u32 %0, %12, %24;\n\t"
+        "addc.cc.u32 %1, %13, %25;\n\t"
+        "addc.cc.u32 %2, %14, %26;\n\t"
+        "addc.cc.u32 %3, %15, %27;\n\t"
+        "addc.cc.u32 %4, %16, %28;\n\t"
+        "addc.cc.u32 %5, %17, %29;\n\t"
+        "addc.cc.u32 %6, %18, %30;\n\t"
+        "addc.cc.u32 %7, %19, %31;\n\t"
+        "addc.cc.u32 %8, %20, %32;\n\t"
+        "addc.cc.u32 %9, %21, 0;\n\t"
+        "addc.cc.u32 %10, %22, 0;\n\t"
+        "addc.u32 %11, %23, 0;\n\t"
+        : "=r"(t[4]), "=r"(t[5]), "=r"(t[6]), "=r"(t[7]), "=r"(t[8]), "=r"(t[9]), "=r"(t[10]), "=r"(t[11]),
+          "=r"(t[12]), "=r"(t[13]), "=r"(t[14]), "=r"(t[15])
+        : "r"(lo[4]), "r"(lo[5]), "r"(lo[6]), "r"(lo[7]), "r"(hi[0]), "r"(hi[1]), "r"(hi[2]), "r"(hi[3]),
+          "r"(hi[4]), "r"(hi[5]), "r"(hi[6]), "r"(hi[7]), "r"(mid[0]), "r"(mid[1]), "r"(mid[2]), "r"(mid[3]),
+          "r"(mid[4]), "r"(mid[5]), "r"(mid[6]), "r"(mid[7]), "r"(mid[8]));
+    return fe_reduce512(t);
+}
+
+#ifndef MK32_KARATSUBA
+#define MK32_KARATSUBA 0
+#endif
+
+// r = a·b mod p (as a value below 2^256)
+__device__ __forceinline__ fe fe_mul(const fe& a, const fe& b) {
+#if MK32_KARATSUBA
+    return fe_mul_karatsuba(a, b);
+#else
+    return fe_mul_schoolbook(a, b);
+#endif
 }
 
 // r = a^2 mod p: the 28 cross products a_i·a_j (i < j) in per-row carry chains (row i
