@@ -701,7 +701,10 @@ def measure(args, workload, steps, e2e_steps, dist, world, rank, local, cpu_seco
                            "multiply, independent accumulators, full occupancy (mk_measure_mad_peaks)",
             "peak_mad_lo": peak_lo / 1e12,
             "frac_of_mad_lo": achieved / (peak_lo / 1e12) if peak_lo else None,
-            "work_per_key": {"field_muls": field_muls, "int_mads": mads_per_key},
+            "work_per_key": {"field_muls": field_muls, "int_mads": mads_per_key,
+                             "mul_form": ("schoolbook: 144 MADs a multiplication" if source == 2 else
+                                          "Karatsuba: 112 MADs a multiplication (comb, batch, back-sweep); "
+                                          "pooled inversions schoolbook (144), squarings 88")},
             # the peak's pieces, each on independent chains or carry-linked rows (Tmad/s)
             "imad_pieces": {k: v / 1e12 for k, v in pieces.items()} if pieces else None,
             "kernel_ms_per_launch": ms_local / (steps * launches),
@@ -801,12 +804,15 @@ def run_autotune(args):
     # the field radix: the search kernel is built for radix 2^32; the others are timed here
     with mk.Context(device=0, table_rows=16, keys_per_thread=8) as c:
         r32, r26, r51 = c.measure_field_mul()
+        forms = c.measure_field_mul_forms()
     best, results = autotune(0, cands, finalists=4, trial_keys=args.tune_keys,
                              job=(workload_key(args.workload), wl["source"], workload_needles(args.workload)))
     for r in results:
         print(json.dumps(r), flush=True)
     print(json.dumps({"workload": args.workload, "best": best, "candidates": len(cands),
-                      "field_mul_per_s": {"radix_2^32": r32, "radix_2^25.5": r26, "radix_2^51_fp64": r51}}),
+                      "field_mul_per_s": {"radix_2^32": r32, "radix_2^25.5": r26, "radix_2^51_fp64": r51,
+                                          "radix_2^32_schoolbook": forms["schoolbook"],
+                                          "radix_2^32_karatsuba": forms["karatsuba"]}}),
           flush=True)
     return 0
 

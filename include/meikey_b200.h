@@ -418,6 +418,13 @@ MK_API int mk_autotune_job(int device, mk_tune_entry* entries, uint32_t n, uint3
 MK_API int mk_measure_field_mul(mk_ctx* ctx, double* radix32_per_s, double* radix26_per_s,
                                 double* radix51_fp64_per_s);
 
+/* Field multiplications per second of the two radix-2^32 forms, measured like
+ * mk_measure_field_mul: the schoolbook product (64 mad.lo + 64 mad.hi) and one level of
+ * Karatsuba on the 128-bit halves (48 + 48, plus about 60 adds and logic operations), which
+ * the secure path's comb additions and batches use.  Both forms run the same chains;
+ * MK_ERR_SELF_CHECK if any result differs. */
+MK_API int mk_measure_field_mul_forms(mk_ctx* ctx, double* schoolbook_per_s, double* karatsuba_per_s);
+
 /* OpenSSH output of a found key.  mk_openssh_public writes the authorized_keys line
  * "ssh-ed25519 <base64 blob>[ comment]" (VanityKey::public_openssh, src/model/key.rs:132-139);
  * mk_openssh_private writes the unencrypted openssh-key-v1 private key file of a seed

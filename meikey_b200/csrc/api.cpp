@@ -979,9 +979,12 @@ int mk_job_io_bytes(const mk_job* j, uint64_t* h2d, uint64_t* d2h) {
 int mk_ctx_work_per_key(const mk_ctx* c, int seed_source, double* field_muls, double* int_mads) {
     if (!c || !field_muls || !int_mads || seed_source < MK_SEED_CHACHA20 || seed_source > MK_SEED_INCREMENTAL)
         return MK_ERR_BAD_ARG;
-    // radix-2^32 costs: a multiplication is 64 mad.lo + 64 mad.hi (8x8 limbs) + 16 (fold by 38),
-    // a squaring 28 cross products + 8 diagonal ones (72) + 16
-    const double MUL = 144.0, SQ = 88.0;
+    // radix-2^32 costs: a schoolbook multiplication is 64 mad.lo + 64 mad.hi (8x8 limbs) + 16
+    // (fold by 38), the Karatsuba form 48 + 48 + 16, a squaring 28 cross products + 8 diagonal
+    // ones (72) + 16.  The secure path's comb, batch and back-sweep multiply in the Karatsuba
+    // form; the incremental path and the pooled inversions in the schoolbook one.
+    const double MUL = mkb::MADS_MUL_SCHOOLBOOK, SQ = mkb::MADS_SQUARE;
+    const double PATH_MUL = seed_source == MK_SEED_INCREMENTAL ? MUL : mkb::MADS_MUL_KARATSUBA;
     const double kpt = c->kpt, rows = c->geom.rows;
     const double ct = mkb::search_threads(c->block, c->layout);
     // comb: row 0 is free, full additions cost 7 multiplications, the last one 3
@@ -1001,7 +1004,7 @@ int mk_ctx_work_per_key(const mk_ctx* c, int seed_source, double* field_muls, do
     double pool_mul = pools * (3.0 * (groups - 1) + 11.0) / (ct * kpt);
     double pool_sq = pools * 254.0 / (ct * kpt);
     *field_muls = comb + batch + pool_mul + pool_sq;
-    *int_mads = (comb + batch + pool_mul) * MUL + pool_sq * SQ;
+    *int_mads = (comb + batch) * PATH_MUL + pool_mul * MUL + pool_sq * SQ;
     return MK_OK;
 }
 
@@ -1140,6 +1143,15 @@ int mk_measure_field_mul(mk_ctx* c, double* radix32_per_s, double* radix26_per_s
     MK_CUDA(c, mkb::measure_field_mul_rates((int)c->info.sms, c->stream, radix32_per_s, radix26_per_s,
                                             radix51_fp64_per_s, &exact));
     if (!exact) return fail(c, MK_ERR_SELF_CHECK, "radix-2^51 (FP64) products differ from radix 2^32");
+    return MK_OK;
+} MK_ABI_CATCH(c ? &c->err : nullptr)
+
+int mk_measure_field_mul_forms(mk_ctx* c, double* schoolbook_per_s, double* karatsuba_per_s) try {
+    if (!c || !schoolbook_per_s || !karatsuba_per_s) return MK_ERR_BAD_ARG;
+    MK_CUDA(c, cudaSetDevice(c->device));
+    bool same = false;
+    MK_CUDA(c, mkb::measure_field_mul_forms((int)c->info.sms, c->stream, schoolbook_per_s, karatsuba_per_s, &same));
+    if (!same) return fail(c, MK_ERR_SELF_CHECK, "Karatsuba field products differ from the schoolbook ones");
     return MK_OK;
 } MK_ABI_CATCH(c ? &c->err : nullptr)
 

@@ -260,19 +260,21 @@ __device__ __forceinline__ fe fe_mul_karatsuba(const fe& a, const fe& b) {
     // the true value A0·B1 + A1·B0 lies in [0, 2^257)
 #pragma unroll
     for (int i = 0; i < 8; i++) mm[i] ^= s;
-    u32 scratch;
-    asm("add.cc.u32 %9, %10, %10;\n\t"
-        "addc.cc.u32 %0, %0, %11;\n\t"
-        "addc.cc.u32 %1, %1, %12;\n\t"
-        "addc.cc.u32 %2, %2, %13;\n\t"
-        "addc.cc.u32 %3, %3, %14;\n\t"
-        "addc.cc.u32 %4, %4, %15;\n\t"
-        "addc.cc.u32 %5, %5, %16;\n\t"
-        "addc.cc.u32 %6, %6, %17;\n\t"
-        "addc.cc.u32 %7, %7, %18;\n\t"
-        "addc.u32 %8, %8, %10;\n\t"
+    asm("{\n\t"
+        ".reg .u32 cf;\n\t"
+        "add.cc.u32 cf, %9, %9;\n\t"
+        "addc.cc.u32 %0, %0, %10;\n\t"
+        "addc.cc.u32 %1, %1, %11;\n\t"
+        "addc.cc.u32 %2, %2, %12;\n\t"
+        "addc.cc.u32 %3, %3, %13;\n\t"
+        "addc.cc.u32 %4, %4, %14;\n\t"
+        "addc.cc.u32 %5, %5, %15;\n\t"
+        "addc.cc.u32 %6, %6, %16;\n\t"
+        "addc.cc.u32 %7, %7, %17;\n\t"
+        "addc.u32 %8, %8, %9;\n\t"
+        "}"
         : "+r"(mid[0]), "+r"(mid[1]), "+r"(mid[2]), "+r"(mid[3]), "+r"(mid[4]), "+r"(mid[5]), "+r"(mid[6]),
-          "+r"(mid[7]), "+r"(mid[8]), "=r"(scratch)
+          "+r"(mid[7]), "+r"(mid[8])
         : "r"(s), "r"(mm[0]), "r"(mm[1]), "r"(mm[2]), "r"(mm[3]), "r"(mm[4]), "r"(mm[5]), "r"(mm[6]), "r"(mm[7]));
     // t = L + mid·2^128 + H·2^256 (below 2^512: no carry out of word 15)
     u32 t[16];
@@ -300,17 +302,15 @@ __device__ __forceinline__ fe fe_mul_karatsuba(const fe& a, const fe& b) {
     return fe_reduce512(t);
 }
 
-#ifndef MK32_KARATSUBA
-#define MK32_KARATSUBA 0
-#endif
-
 // r = a·b mod p (as a value below 2^256)
-__device__ __forceinline__ fe fe_mul(const fe& a, const fe& b) {
-#if MK32_KARATSUBA
-    return fe_mul_karatsuba(a, b);
-#else
-    return fe_mul_schoolbook(a, b);
-#endif
+__device__ __forceinline__ fe fe_mul(const fe& a, const fe& b) { return fe_mul_schoolbook(a, b); }
+
+// r = a·b mod p in the form a kernel picks at compile time: Karatsuba when K.  Both forms
+// return the same words for the same inputs.
+template <bool K>
+__device__ __forceinline__ fe fe_mul_as(const fe& a, const fe& b) {
+    if constexpr (K) return fe_mul_karatsuba(a, b);
+    else return fe_mul_schoolbook(a, b);
 }
 
 // r = a^2 mod p: the 28 cross products a_i·a_j (i < j) in per-row carry chains (row i

@@ -29,28 +29,31 @@ __device__ __forceinline__ void fe_cswap(fe& a, fe& b, bool swap) {
 
 // P + Q for a table point Q given with its digit sign: a negative digit uses -Q,
 // which swaps y+x / y-x and flips the sign of the 2dxy term (so F and G trade places).
+// K: the field multiplies in Karatsuba form (same results).
+template <bool K = false>
 __device__ __forceinline__ ge ge_add_niels(const ge& p, niels q, bool neg) {
     fe_cswap(q.ypx, q.ymx, neg);
-    fe a = fe_mul(fe_sub(p.Y, p.X), q.ymx);
-    fe b = fe_mul(fe_add(p.Y, p.X), q.ypx);
-    fe c = fe_mul(p.T, q.t2d);
+    fe a = fe_mul_as<K>(fe_sub(p.Y, p.X), q.ymx);
+    fe b = fe_mul_as<K>(fe_add(p.Y, p.X), q.ypx);
+    fe c = fe_mul_as<K>(p.T, q.t2d);
     fe d = fe_add(p.Z, p.Z);
     fe e = fe_sub(b, a), h = fe_add(b, a);
     fe f = fe_sub(d, c), g = fe_add(d, c);
     fe_cswap(f, g, neg);
     ge r;
-    r.X = fe_mul(e, f);
-    r.Y = fe_mul(g, h);
-    r.Z = fe_mul(f, g);
-    r.T = fe_mul(e, h);
+    r.X = fe_mul_as<K>(e, f);
+    r.Y = fe_mul_as<K>(g, h);
+    r.Z = fe_mul_as<K>(f, g);
+    r.T = fe_mul_as<K>(e, h);
     return r;
 }
 
 // Last addition (digit >= 0): the sum's y as a fraction yn/yd and, optionally, x as xn/xd.
+template <bool K = false>
 __device__ __forceinline__ void ge_add_niels_frac(const ge& p, const niels& q, fe& yn, fe& yd, fe* xn, fe* xd) {
-    fe a = fe_mul(fe_sub(p.Y, p.X), q.ymx);
-    fe b = fe_mul(fe_add(p.Y, p.X), q.ypx);
-    fe c = fe_mul(p.T, q.t2d);
+    fe a = fe_mul_as<K>(fe_sub(p.Y, p.X), q.ymx);
+    fe b = fe_mul_as<K>(fe_add(p.Y, p.X), q.ypx);
+    fe c = fe_mul_as<K>(p.T, q.t2d);
     fe d = fe_add(p.Z, p.Z);
     yn = fe_add(b, a);
     yd = fe_sub(d, c);

@@ -28,6 +28,12 @@ using mk32::niels;
 using mk32::u32;
 using mk32::u64;
 
+// Field-multiply form of the secure path (comb additions, thread batches and back-sweep): one
+// level of Karatsuba, 48 lo + 48 hi products a multiplication instead of 64 + 64, with the same
+// results.  On B200 it is the faster form there; the incremental path, with few multiplies
+// between its other work, runs faster with the schoolbook form and keeps it.
+constexpr bool SECURE_KARATSUBA = true;
+
 // ---------------------------------------------------------------------------
 // shared helpers
 // ---------------------------------------------------------------------------
@@ -201,11 +207,11 @@ __device__ __forceinline__ void comb_mul(const uint4* __restrict__ table, const 
         fetch_entry(slot, (row + 1) & 1, table, entry_index(g, row + 1, dn));
         wait_entries<1>();
         niels n = read_entry(slot, row & 1);
-        P = mk32::ge_add_niels(P, n, d < 0);
+        P = mk32::ge_add_niels<SECURE_KARATSUBA>(P, n, d < 0);
     }
     wait_entries<0>();
     niels n = read_entry(slot, (rows - 1) & 1);
-    mk32::ge_add_niels_frac(P, n, yn, yd, xn, xd);
+    mk32::ge_add_niels_frac<SECURE_KARATSUBA>(P, n, yn, yd, xn, xd);
 }
 
 // comb_mul with one 8-round step of the SHA-512 `run` (the next iteration's seed) in every
@@ -239,11 +245,11 @@ __device__ __forceinline__ void comb_mul_sha(const uint4* __restrict__ table, co
         wait_entries<1>();
         niels n = read_entry(slot, row & 1);
         mkh::sha_run_step(run, 8u * (row - 1));
-        P = mk32::ge_add_niels(P, n, d < 0);
+        P = mk32::ge_add_niels<SECURE_KARATSUBA>(P, n, d < 0);
     }
     wait_entries<0>();
     niels n = read_entry(slot, (rows - 1) & 1);
-    mk32::ge_add_niels_frac(P, n, yn, yd, nullptr, nullptr);
+    mk32::ge_add_niels_frac<SECURE_KARATSUBA>(P, n, yn, yd, nullptr, nullptr);
 }
 
 // 6-bit values of the 44-character base64 tail of the key blob (0x20 then the key),
@@ -447,11 +453,11 @@ __device__ __forceinline__ void comb_mul_smem(const uint4* stab, const CombGeom&
 #pragma unroll 1
     for (u32 row = 1; row + 1 < rows; row++) {
         d = next_digit(g, m, row, carry);
-        P = mk32::ge_add_niels(P, smem_niels(stab + entry_index(g, row, d) * 6), d < 0);
+        P = mk32::ge_add_niels<SECURE_KARATSUBA>(P, smem_niels(stab + entry_index(g, row, d) * 6), d < 0);
     }
     // the top row's digit is unsigned: the carry lands in it unchanged
     d = (int)bits_at(m, g.offset[rows - 1], g.width[rows - 1]) + carry;
-    mk32::ge_add_niels_frac(P, smem_niels(stab + entry_index(g, rows - 1, d) * 6), yn, yd, nullptr, nullptr);
+    mk32::ge_add_niels_frac<SECURE_KARATSUBA>(P, smem_niels(stab + entry_index(g, rows - 1, d) * 6), yn, yd, nullptr, nullptr);
 }
 
 // Comb multiplies of the KPT scalars (IMAD work) into the batch; STAB: from the table in
@@ -469,8 +475,8 @@ __device__ __forceinline__ void combs(const KeyLaunch& L, const CombGeom& g, con
             b.a[0] = num;
             run = b.den[0];
         } else {
-            b.a[j] = mk32::fe_mul(num, run);
-            run = mk32::fe_mul(run, b.den[j]);
+            b.a[j] = mk32::fe_mul_as<SECURE_KARATSUBA>(num, run);
+            run = mk32::fe_mul_as<SECURE_KARATSUBA>(run, b.den[j]);
         }
     }
     b.prod = run;
@@ -520,23 +526,24 @@ __device__ __forceinline__ void combs_sha(const KeyLaunch& L, const CombGeom& g,
             b.a[0] = num;
             run = b.den[0];
         } else {
-            b.a[j] = mk32::fe_mul(num, run);
-            run = mk32::fe_mul(run, b.den[j]);
+            b.a[j] = mk32::fe_mul_as<SECURE_KARATSUBA>(num, run);
+            run = mk32::fe_mul_as<SECURE_KARATSUBA>(run, b.den[j]);
         }
     }
     b.prod = run;
 }
 
 // Backward pass: `inv` is 1/(product of the batch's denominators); yields each key's
-// canonical y (sign bit 0), tests the needles and reports candidate hits.
-template <int KPT>
+// canonical y (sign bit 0), tests the needles and reports candidate hits.  K: Karatsuba
+// multiplies.
+template <int KPT, bool K = false>
 __device__ __forceinline__ void backward(const KeyLaunch& L, const MatchSet& ms, const u32* lane_masks, u64 first,
                                          const Batch<KPT>& b, fe inv, u32& sink) {
 #pragma unroll 1
     for (int j = KPT - 1; j >= 0; j--) {
         u32 pk[8];
-        mk32::fe_to_words(mk32::fe_mul(b.a[j], inv), pk);
-        if (j > 0) inv = mk32::fe_mul(inv, b.den[j]);
+        mk32::fe_to_words(mk32::fe_mul_as<K>(b.a[j], inv), pk);
+        if (j > 0) inv = mk32::fe_mul_as<K>(inv, b.den[j]);
         sink ^= pk[7];
         u64 hw[2];
         match_key(ms, lane_masks, pk, hw);
@@ -812,7 +819,8 @@ __global__ void __launch_bounds__(BLOCK, 512 / BLOCK) k_search(const KeyLaunch L
         const int b = it & 1;
         if (it + 1 < iters && it + 1 < stop_iter) produce(it + 1);
         if (!inverts(it)) bar_sync(3 + b, BLOCK);
-        backward<KPT>(L, ms, ms.narrow ? lane_masks : nullptr, first_of(it), batch[b], prod[b][tid], sink);
+        backward<KPT, !INCR && SECURE_KARATSUBA>(L, ms, ms.narrow ? lane_masks : nullptr, first_of(it), batch[b],
+                                                 prod[b][tid], sink);
         if (it + 1 >= iters || it + 1 >= stop_iter) break;
     }
     // warp 0 never inverts, so with ROT the last stop decision is visible here
@@ -972,8 +980,8 @@ __global__ void __launch_bounds__(BLOCK, 1) k_search_hw(const KeyLaunch L) {
                 bt.a[0] = num;
                 run = bt.den[0];
             } else {
-                bt.a[j] = mk32::fe_mul(num, run);
-                run = mk32::fe_mul(run, bt.den[j]);
+                bt.a[j] = mk32::fe_mul_as<SECURE_KARATSUBA>(num, run);
+                run = mk32::fe_mul_as<SECURE_KARATSUBA>(run, bt.den[j]);
             }
         }
         bt.prod = run;
@@ -985,7 +993,8 @@ __global__ void __launch_bounds__(BLOCK, 1) k_search_hw(const KeyLaunch L) {
         const int b = it & 1;
         if (it + 1 < iters && it + 1 < stop_iter) produce(it + 1);
         bar_sync(3 + b, B_PIPE);
-        backward<KPT>(L, ms, ms.narrow ? lane_masks : nullptr, first_of(it, gid), batch[b], prod[b][tid], sink);
+        backward<KPT, SECURE_KARATSUBA>(L, ms, ms.narrow ? lane_masks : nullptr, first_of(it, gid), batch[b],
+                                        prod[b][tid], sink);
         if (it + 1 >= iters || it + 1 >= stop_iter) break;
     }
     if (L.sink) L.sink[gid] = sink;
@@ -1403,7 +1412,8 @@ namespace mkb {
 // 2^25.5 (fe26.cuh, ten limbs, 100 mad.wide products) and radix 2^51 in FP64 registers
 // (fe51.cuh, five limbs, products split by fused multiply-adds) are the alternatives the
 // search is not built for.  Radices 32 and 51 start from the same words and write the XOR
-// of their chains' canonical words, so their outputs must agree.
+// of their chains' canonical words, so their outputs must agree.  RADIX 33 is radix 2^32 with
+// the Karatsuba multiply (fe_mul_karatsuba), which must agree with the schoolbook form too.
 template <int RADIX>
 __global__ void __launch_bounds__(256) k_fe_mul_rate(uint32_t iters, uint32_t seed, uint32_t* out) {
     uint32_t sum = 0;
@@ -1414,13 +1424,13 @@ __global__ void __launch_bounds__(256) k_fe_mul_rate(uint32_t iters, uint32_t se
     for (int q = 0; q < 4; q++)
 #pragma unroll
         for (int i = 0; i < 8; i++) wa[q][i] = threadIdx.x * 7 + q * 8 + i;
-    if (RADIX == 32) {
+    if (RADIX == 32 || RADIX == 33) {
         mk32::fe a[4], b = mk32::fe_from_words(wb);
 #pragma unroll
         for (int q = 0; q < 4; q++) a[q] = mk32::fe_from_words(wa[q]);
         for (uint32_t it = 0; it < iters; it++)
 #pragma unroll
-            for (int q = 0; q < 4; q++) a[q] = mk32::fe_mul(a[q], b);
+            for (int q = 0; q < 4; q++) a[q] = mk32::fe_mul_as<RADIX == 33>(a[q], b);
 #pragma unroll
         for (int q = 0; q < 4; q++) {
             uint32_t w[8];
@@ -1510,6 +1520,57 @@ cudaError_t measure_field_mul_rates(int sms, cudaStream_t st, double* radix32_pe
     *radix26_per_s = best[1];
     *radix51_per_s = best[2];
     *radix51_exact = same;
+    return e;
+}
+
+// Rates of the two radix-2^32 multiplication forms (schoolbook and Karatsuba), measured like
+// measure_field_mul_rates, and whether their chains end in the same words.
+cudaError_t measure_field_mul_forms(int sms, cudaStream_t st, double* schoolbook_per_s, double* karatsuba_per_s,
+                                    bool* same_words) {
+    const uint32_t blocks = (uint32_t)sms * 8, threads = 256, iters = 1u << 11;
+    const size_t n = (size_t)blocks * threads;
+    uint32_t* out = nullptr;
+    cudaError_t e = cudaMalloc(&out, sizeof(uint32_t) * n * 2);
+    if (e != cudaSuccess) return e;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    double best[2] = {0, 0};
+    auto launch = [&](int k, uint32_t it, uint32_t seed, uint32_t* o) {
+        if (k == 0) k_fe_mul_rate<32><<<blocks, threads, 0, st>>>(it, seed, o);
+        else k_fe_mul_rate<33><<<blocks, threads, 0, st>>>(it, seed, o);
+    };
+    for (int k = 0; k < 2; k++) launch(k, iters / 16, 5u, out);
+    for (int rep = 0; rep < 8 && e == cudaSuccess; rep++) {
+        const int k = rep & 1;
+        cudaEventRecord(e0, st);
+        launch(k, iters, 9u + rep, out);
+        cudaEventRecord(e1, st);
+        e = cudaEventSynchronize(e1);
+        if (e == cudaSuccess) e = cudaGetLastError();
+        float ms = 0;
+        if (e == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+        const double muls = (double)n * iters * 4;
+        if (ms > 0 && muls / (ms * 1e-3) > best[k]) best[k] = muls / (ms * 1e-3);
+    }
+    bool same = false;
+    if (e == cudaSuccess) {
+        launch(0, 97, 3u, out);
+        launch(1, 97, 3u, out + n);
+        e = cudaStreamSynchronize(st);
+        if (e == cudaSuccess) e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) {
+        std::vector<uint32_t> h(n * 2);
+        e = cudaMemcpy(h.data(), out, sizeof(uint32_t) * n * 2, cudaMemcpyDeviceToHost);
+        same = e == cudaSuccess && std::equal(h.begin(), h.begin() + n, h.begin() + n);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(out);
+    *schoolbook_per_s = best[0];
+    *karatsuba_per_s = best[1];
+    *same_words = same;
     return e;
 }
 

@@ -66,6 +66,15 @@ cudaError_t launch_keys(const KeyLaunch& L, bool derive, uint32_t kpt, uint32_t 
 // radix 2^51 in FP64; *radix51_exact tells whether radix-2^51 chains matched radix 2^32.
 cudaError_t measure_field_mul_rates(int sms, cudaStream_t st, double* radix32_per_s, double* radix26_per_s,
                                     double* radix51_per_s, bool* radix51_exact);
+// Field multiplications per second of the schoolbook and Karatsuba radix-2^32 forms;
+// *same_words tells whether their chains ended in the same words.
+cudaError_t measure_field_mul_forms(int sms, cudaStream_t st, double* schoolbook_per_s, double* karatsuba_per_s,
+                                    bool* same_words);
+// Integer multiply-adds of one radix-2^32 field multiplication in each form (products and the
+// fold by 38) and of a squaring; the secure path multiplies in the Karatsuba form.
+constexpr double MADS_MUL_SCHOOLBOOK = 64 + 64 + 16;
+constexpr double MADS_MUL_KARATSUBA = 48 + 48 + 16;
+constexpr double MADS_SQUARE = 72 + 16;
 // The kernel of a variant and its dynamic shared memory (for graph nodes); sets the
 // kernel's shared-memory limit like launch_keys does.
 cudaError_t keys_kernel(bool derive, bool incr, uint32_t kpt, uint32_t block, uint32_t layout, uint32_t dfa_smem,

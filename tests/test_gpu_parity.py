@@ -439,6 +439,13 @@ def test_field_mul_rates(gpu_ctx):
     assert r32 > 1e10 and r26 > 1e10 and r51 > 1e10
 
 
+def test_field_mul_forms(gpu_ctx):
+    """Both radix-2^32 multiplication forms run, and the Karatsuba chains end in the same words
+    as the schoolbook ones (checked inside the call, which raises on a difference)."""
+    r = gpu_ctx.measure_field_mul_forms()
+    assert r["schoolbook"] > 1e10 and r["karatsuba"] > 1e10
+
+
 def test_incremental_range_must_not_wrap(gpu_ctx):
     """Incremental indices are scalar offsets: ranges that would wrap past 2^64 are refused."""
     s0 = _start_scalar(0)
