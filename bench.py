@@ -50,7 +50,7 @@ WORKLOADS = {
     # the reference's published GPU mode (docs/benchmark.md): low-security counter seeds, the
     # needle TARGET case-insensitive
     "counter": {"total": 1 << 33, "step": 1 << 30, "source": 1, "seed": 7, "length": 0, "mode": "contains_ci",
-                "needle": "TARGET", "kpt": 4},
+                "needle": "TARGET", "kpt": 8},
     "incremental": {"total": 1 << 32, "step": 1 << 28, "source": 2, "seed": 11, "length": 6, "mode": "suffix"},
     "multi": {"total": 1 << 34, "step": 1 << 30, "source": 0, "seed": 23, "length": 0, "mode": "mixed",
               "launches": 4, "inverter_rotates": True, "kpt": 16, "inversion_batch": 256},

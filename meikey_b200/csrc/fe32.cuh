@@ -230,15 +230,18 @@ __device__ __forceinline__ u32 absdiff128(const u32 x[4], const u32 y[4], u32 d[
 }
 
 // r = a·b mod p by one level of subtractive Karatsuba on the 128-bit halves
-// (a = A1·2^128 + A0): A0·B1 + A1·B0 = L + H ± |A0 - A1|·|B1 - B0| with L = A0·B0 and
+// (a = A1·2^128 + A0): A0·B1 + A1·B0 = L + H - (A0 - A1)·(B0 - B1) with L = A0·B0 and
 // H = A1·B1, so the 512-bit product takes 48 lo + 48 hi products and about 60 adds and
-// logic operations instead of 64 + 64.  The product t is the same 512-bit integer as the
+// logic operations instead of 64 + 64.  Both operands use the same difference X0 - X1, so an
+// operand that enters several products (the point-addition outputs' E, F, G, H) has one
+// |X0 - X1| the compiler can share.  The product t is the same 512-bit integer as the
 // schoolbook's, and so is the folded result.
 __device__ __forceinline__ fe fe_mul_karatsuba(const fe& a, const fe& b) {
     u32 da[4], db[4], mm[8], lo[8], hi[8], mid[9];
     const u32 sa = absdiff128(&a.v[0], &a.v[4], da);
-    const u32 sb = absdiff128(&b.v[4], &b.v[0], db);
-    const u32 s = sa ^ sb;  // all ones: the middle product is subtracted
+    const u32 sb = absdiff128(&b.v[0], &b.v[4], db);
+    // (A0 - A1)(B0 - B1) is subtracted, so |..|·|..| is subtracted when the signs agree
+    const u32 s = ~(sa ^ sb);  // all ones: the middle product is subtracted
     mul128(da, db, mm);
     mul128(&a.v[0], &b.v[0], lo);
     mul128(&a.v[4], &b.v[4], hi);
