@@ -391,6 +391,16 @@ MK_API int mk_derive_noalloc(mk_ctx* ctx, const uint8_t key[32], int seed_source
 MK_API int mk_regex_compile(const char* pattern, int case_sensitive, uint32_t max_states, uint8_t* table,
                             uint32_t* states, char* err, size_t err_size);
 
+/* mk_regex_compile with the subset construction (the part of Dfa::new whose cost grows with
+ * the DFA) on the context's GPU: the host parses the pattern and builds its NFA and each NFA
+ * state's epsilon closures, then one CTA walks the DFA breadth first, resolving the successors
+ * of a frontier's (state, value) pairs in parallel and numbering new states in the host's
+ * order.  The table, state count, status and error text are those of mk_regex_compile for the
+ * same arguments.  NFAs of up to 2048 states (MK_ERR_PATTERN beyond).  Runs on the context's
+ * stream and waits for it. */
+MK_API int mk_regex_compile_device(mk_ctx* ctx, const char* pattern, int case_sensitive, uint32_t max_states,
+                                   uint8_t* table, uint32_t* states, char* err, size_t err_size);
+
 /* Staged autotuner (GpuOptions::fastest_staged, src/service/gpu.rs:302-393, 1016-1113):
  * stage 1 creates a self-checked context per candidate (a variant whose keys differ from the
  * host derivation is dropped) and times one launch of about trial_keys secure-path

@@ -156,6 +156,9 @@ SIGNATURES = [
                                             ctypes.POINTER(ctypes.c_double)]),
     ("mk_regex_compile", ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_uint32, ctypes.c_void_p,
                                         ctypes.POINTER(ctypes.c_uint32), ctypes.c_char_p, ctypes.c_size_t]),
+    ("mk_regex_compile_device", ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_uint32,
+                                               ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint32), ctypes.c_char_p,
+                                               ctypes.c_size_t]),
     ("mk_autotune", ctypes.c_int, [ctypes.c_int, ctypes.POINTER(TuneEntryC), ctypes.c_uint32, ctypes.c_uint32,
                                    ctypes.c_uint64, ctypes.POINTER(ctypes.c_uint32)]),
     ("mk_autotune_job", ctypes.c_int, [ctypes.c_int, ctypes.POINTER(TuneEntryC), ctypes.c_uint32, ctypes.c_uint32,

@@ -14,9 +14,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(CSRC, "_build")
 LIB = os.path.join(HERE, "libmeikey_b200.so")
-SOURCES = ["kernels.cu", "api.cpp", "host25519.cpp", "regex.cpp", "tune.cpp", "serve.cpp", "keyfile.cpp"]
+SOURCES = ["kernels.cu", "dfa_build.cu", "api.cpp", "host25519.cpp", "regex.cpp", "tune.cpp", "serve.cpp",
+           "keyfile.cpp"]
 HEADERS = ["fe32.cuh", "fe26.cuh", "fe51.cuh", "ge.cuh", "hash.cuh", "kernels.h", "types.h", "host25519.h", "hitsort.h",
-           "abi_guard.h", "jobs.h"]
+           "abi_guard.h", "jobs.h", "regex.h"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMPILE_FLAGS = ARCH + ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC,-O2,-fvisibility=hidden"]

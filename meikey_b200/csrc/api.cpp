@@ -23,6 +23,7 @@
 #include "host25519.h"
 #include "jobs.h"
 #include "kernels.h"
+#include "regex.h"
 
 using mkb::CombGeom;
 
@@ -1143,6 +1144,33 @@ int mk_measure_field_mul(mk_ctx* c, double* radix32_per_s, double* radix26_per_s
     MK_CUDA(c, mkb::measure_field_mul_rates((int)c->info.sms, c->stream, radix32_per_s, radix26_per_s,
                                             radix51_fp64_per_s, &exact));
     if (!exact) return fail(c, MK_ERR_SELF_CHECK, "radix-2^51 (FP64) products differ from radix 2^32");
+    return MK_OK;
+} MK_ABI_CATCH(c ? &c->err : nullptr)
+
+int mk_regex_compile_device(mk_ctx* c, const char* pattern, int case_sensitive, uint32_t max_states, uint8_t* table,
+                            uint32_t* states, char* err, size_t err_size) try {
+    auto error = [&](const std::string& m, int code) {
+        if (err && err_size) snprintf(err, err_size, "%s", m.c_str());
+        return code;
+    };
+    if (err && err_size) err[0] = 0;
+    if (!c || !pattern || !table || !states || max_states < 2 || max_states > 65535)
+        return error("bad argument", MK_ERR_BAD_ARG);
+    *states = 0;
+    mkre::NfaTables t;
+    std::string msg;
+    int st = mkre::nfa_tables(pattern, case_sensitive, mkb::MAX_DFA_NFA_WORDS, &t, &msg);
+    if (st != MK_OK) return error(msg, st);
+    MK_CUDA(c, cudaSetDevice(c->device));
+    std::vector<uint8_t> rows;
+    uint32_t n = 0;
+    bool too_many = false;
+    MK_CUDA(c, mkb::build_dfa_device(t, max_states, c->stream, &rows, &n, &too_many));
+    if (too_many) return error(mkre::too_complex(max_states), MK_ERR_PATTERN);
+    st = mkre::check_table(rows.data(), n, &msg);
+    if (st != MK_OK) return error(msg, st);
+    memcpy(table, rows.data(), (size_t)n * 130);
+    *states = n;
     return MK_OK;
 } MK_ABI_CATCH(c ? &c->err : nullptr)
 

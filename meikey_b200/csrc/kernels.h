@@ -3,7 +3,13 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <vector>
+
 #include "types.h"
+
+namespace mkre {
+struct NfaTables;
+}
 
 namespace mkb {
 
@@ -66,6 +72,13 @@ cudaError_t launch_keys(const KeyLaunch& L, bool derive, uint32_t kpt, uint32_t 
 // radix 2^51 in FP64; *radix51_exact tells whether radix-2^51 chains matched radix 2^32.
 cudaError_t measure_field_mul_rates(int sms, cudaStream_t st, double* radix32_per_s, double* radix26_per_s,
                                     double* radix51_per_s, bool* radix51_exact);
+// Subset construction of a regex DFA on the device (dfa_build.cu) from the pattern's NFA
+// tables: the table of mk_regex_compile (states x 65 u16, row 0 the accept state) in *table
+// and its state count in *states, or *too_many when it has more than max_states states.
+// Synchronizes `st`.  NFAs of up to 32·MAX_DFA_NFA_WORDS states.
+constexpr uint32_t MAX_DFA_NFA_WORDS = 64;
+cudaError_t build_dfa_device(const mkre::NfaTables& t, uint32_t max_states, cudaStream_t st,
+                             std::vector<uint8_t>* table, uint32_t* states, bool* too_many);
 // Field multiplications per second of the schoolbook and Karatsuba radix-2^32 forms;
 // *same_words tells whether their chains ended in the same words.
 cudaError_t measure_field_mul_forms(int sms, cudaStream_t st, double* schoolbook_per_s, double* karatsuba_per_s,

@@ -41,6 +41,7 @@
 #include <vector>
 
 #include "../../include/meikey_b200.h"
+#include "regex.h"
 
 namespace {
 
@@ -692,7 +693,102 @@ double table_probability(const std::vector<std::vector<uint32_t>>& trans, const 
     return p;
 }
 
+const char NO_MATCH[] =
+    "no public key matches this regular expression (the characters are A-Z a-z 0-9 + /, and the one right "
+    "after the fixed part is A-P)";
+
+// Parses `pattern`, applies the pattern checks and builds its NFA; throws Error.
+void build_nfa(const std::string& pattern, bool fold, Nfa& nfa, int& start, int& match) {
+    if (pattern.empty()) throw Error{"the pattern is empty"};
+    Parser p(pattern, fold);
+    Node ast = p.parse();
+    if (min_len(ast) == 0) throw Error{"the pattern matches the empty string"};
+    start = nfa.add();
+    match = nfa.add();
+    nfa.build(ast, start, match);
+}
+
 }  // namespace
+
+namespace mkre {
+
+std::string too_complex(uint32_t max_states) {
+    return "the regular expression is too complex (the DFA has more than " + std::to_string(max_states) +
+           " states)";
+}
+
+int check_table(const uint8_t* table, uint32_t states, std::string* err) {
+    std::vector<std::vector<uint32_t>> trans(states, std::vector<uint32_t>(64));
+    std::vector<bool> eoi(states);
+    for (uint32_t st = 0; st < states; st++) {
+        for (int v = 0; v < 65; v++) {
+            const uint32_t x = table[(st * 65 + v) * 2] | (uint32_t)table[(st * 65 + v) * 2 + 1] << 8;
+            if (v < 64) trans[st][v] = x < states ? x : 0;
+            else eoi[st] = x != 0;
+        }
+    }
+    if (states >= 2 && table_probability(trans, eoi) != 0.0) return MK_OK;
+    *err = NO_MATCH;
+    return MK_ERR_PATTERN;
+}
+
+int nfa_tables(const char* pattern, int case_sensitive, uint32_t max_words, NfaTables* out, std::string* err) try {
+    Nfa nfa;
+    int start = 0, match = 0;
+    build_nfa(pattern, case_sensitive == 0, nfa, start, match);
+    const uint32_t n = (uint32_t)nfa.eps.size(), words = (n + 31) / 32;
+    if (words > max_words) {
+        *err = "the pattern is too large for the device DFA builder (" + std::to_string(n) + " NFA states, at most " +
+               std::to_string(32 * max_words) + ")";
+        return MK_ERR_PATTERN;
+    }
+    NfaTables& t = *out;
+    t = NfaTables();
+    t.n = n;
+    t.words = words;
+    t.start = start;
+    t.match = match;
+    t.track_word = nfa.has_word;
+    t.track_start = nfa.has_word && nfa.has_start;
+    std::vector<int> mark(n, 0);
+    int stamp = 0;
+    auto put = [&](const std::vector<int>& set, uint32_t* bits) {
+        for (int x : set) bits[x >> 5] |= 1u << (x & 31);
+    };
+    auto holds_match = [&](const std::vector<int>& set) { return std::binary_search(set.begin(), set.end(), match); };
+    t.k0.assign(words, 0);
+    put(nfa.closure({start}, At{true, false, false, false}, false, mark, stamp), t.k0.data());
+    t.sym_to.assign(nfa.sym_to.begin(), nfa.sym_to.end());
+    t.sym.assign(nfa.sym.begin(), nfa.sym.end());
+    t.plain.assign((size_t)n * words, 0);
+    t.plainm.assign(words, 0);
+    t.decm.assign(8 * (size_t)words, 0);
+    t.endm.assign(4 * (size_t)words, 0);
+    if (t.track_word) t.dec.assign(8 * (size_t)n * words, 0);
+    for (uint32_t x = 0; x < n; x++) {
+        const uint32_t bit = 1u << (x & 31), w = x >> 5;
+        const std::vector<int> pc = nfa.closure({(int)x}, At{false, false, false, false}, false, mark, stamp);
+        put(pc, &t.plain[(size_t)x * words]);
+        if (holds_match(pc)) t.plainm[w] |= bit;
+        for (int c = 0; c < 4; c++) {
+            const At at{(c & 2) != 0, true, (c & 1) != 0, false};
+            if (holds_match(nfa.closure({(int)x}, at, true, mark, stamp))) t.endm[(size_t)c * words + w] |= bit;
+        }
+        if (!t.track_word) continue;
+        for (int c = 0; c < 8; c++) {
+            const At at{(c & 4) != 0, false, (c & 2) != 0, (c & 1) != 0};
+            const std::vector<int> dc = nfa.closure({(int)x}, at, true, mark, stamp);
+            put(dc, &t.dec[((size_t)c * n + x) * words]);
+            if (holds_match(dc)) t.decm[(size_t)c * words + w] |= bit;
+        }
+    }
+    return MK_OK;
+} catch (const Error& e) {
+    *err = e.msg;
+    return MK_ERR_PATTERN;
+}
+
+}  // namespace mkre
 
 extern "C" int mk_regex_compile(const char* pattern, int case_sensitive, uint32_t max_states, uint8_t* table,
                                 uint32_t* states, char* err, size_t err_size) {
@@ -704,14 +800,9 @@ extern "C" int mk_regex_compile(const char* pattern, int case_sensitive, uint32_
     if (!pattern || !table || !states || max_states < 2 || max_states > 65535) return error("bad argument", MK_ERR_BAD_ARG);
     *states = 0;
     try {
-        std::string s(pattern);
-        if (s.empty()) return error("the pattern is empty", MK_ERR_PATTERN);
-        Parser p(s, case_sensitive == 0);
-        Node ast = p.parse();
-        if (min_len(ast) == 0) return error("the pattern matches the empty string", MK_ERR_PATTERN);
         Nfa nfa;
-        int start = nfa.add(), match = nfa.add();
-        nfa.build(ast, start, match);
+        int start = 0, match = 0;
+        build_nfa(pattern, case_sensitive == 0, nfa, start, match);
         std::vector<int> mark(nfa.eps.size(), 0);
         int stamp = 0;
         // a DFA state: NFA states (closed over plain edges and the start assertion where it
@@ -756,10 +847,7 @@ extern "C" int mk_regex_compile(const char* pattern, int case_sensitive, uint32_
                 auto it = ids.find(key);
                 if (it == ids.end()) {
                     uint32_t id = (uint32_t)order.size() + 1;
-                    if (order.size() + 2 > max_states)
-                        return error("the regular expression is too complex (the DFA has more than " +
-                                         std::to_string(max_states) + " states)",
-                                     MK_ERR_PATTERN);
+                    if (order.size() + 2 > max_states) return error(mkre::too_complex(max_states), MK_ERR_PATTERN);
                     ids[key] = id;
                     order.push_back(key);
                     row[v] = id;
@@ -772,10 +860,7 @@ extern "C" int mk_regex_compile(const char* pattern, int case_sensitive, uint32_
             const std::vector<int> E = nfa.closure(S, At{first, true, prev_word, false}, true, mark, stamp);
             eoi.push_back(std::binary_search(E.begin(), E.end(), match));
         }
-        if (table_probability(trans, eoi) == 0.0)
-            return error("no public key matches this regular expression (the characters are A-Z a-z 0-9 + /, "
-                         "and the one right after the fixed part is A-P)",
-                         MK_ERR_PATTERN);
+        if (table_probability(trans, eoi) == 0.0) return error(NO_MATCH, MK_ERR_PATTERN);
         const size_t n = trans.size();
         for (size_t st = 0; st < n; st++) {
             for (int v = 0; v < 65; v++) {

@@ -45,17 +45,27 @@ class Needle:
         return Needle(bytes(table), L.MODE_REGEX, False, states)
 
     @staticmethod
-    def regex(pattern: str, case_sensitive: bool = True, max_states: int = 16384) -> "Needle":
+    def regex(pattern: str, case_sensitive: bool = True, max_states: int = 16384, device: "Context" = None) -> "Needle":
         """A regex needle compiled by the library (mk_regex_compile); max_states defaults to the
-        reference's limit (MAX_STATES, src/model/pattern/dfa.rs:18)."""
+        reference's limit (MAX_STATES, src/model/pattern/dfa.rs:18).  With a context as `device`
+        the subset construction runs on its GPU (mk_regex_compile_device, the same table)."""
         lib = L.load()
         table = ctypes.create_string_buffer(max_states * 130)
         states = ctypes.c_uint32()
         err = ctypes.create_string_buffer(256)
-        st = lib.mk_regex_compile(pattern.encode(), 1 if case_sensitive else 0, max_states, table,
-                                  ctypes.byref(states), err, 256)
+        if device is None:
+            st = lib.mk_regex_compile(pattern.encode(), 1 if case_sensitive else 0, max_states, table,
+                                      ctypes.byref(states), err, 256)
+        else:
+            st = lib.mk_regex_compile_device(device._ptr, pattern.encode(), 1 if case_sensitive else 0, max_states,
+                                             table, ctypes.byref(states), err, 256)
         if st != L.OK:
-            raise GpuError(st, err.value.decode(errors="replace"))
+            msg = err.value.decode(errors="replace")
+            if not msg and device is not None:
+                buf = ctypes.create_string_buffer(512)
+                lib.mk_last_error(device._ptr, buf, 512)
+                msg = buf.value.decode(errors="replace")
+            raise GpuError(st, msg)
         return Needle.dfa(table.raw[:states.value * 130], states.value)
 
     def c_len(self) -> int:
