@@ -33,7 +33,6 @@ struct DfaDev {
     const uint64_t* sym;     // [n]
     uint32_t* keys;          // [max_states][words + 1]: DFA state j + 1 (word `words` holds its flags)
     uint32_t* cand;          // [DFA_CHUNK][words + 1]
-    int32_t* cand_id;        // [DFA_CHUNK]
     uint32_t* hash;          // [hash_mask + 1]: key index + 1, 0 when empty
     uint16_t* table;         // [max_states][65]
     uint32_t* result;        // [0] states including the accept state, [1] 1 when max_states was exceeded
@@ -124,6 +123,8 @@ __device__ int32_t dfa_step(const DfaDev& d, uint32_t k, uint32_t v, uint32_t* o
 __global__ void __launch_bounds__(DFA_BLOCK) k_dfa_build(DfaDev d) {
     __shared__ uint32_t s_count;  // DFA states found, without the accept state
     __shared__ uint32_t s_over;
+    __shared__ int32_t s_id[DFA_CHUNK];         // the chunk's successor ids, -1 while unnumbered
+    __shared__ uint32_t s_new[DFA_CHUNK / 32];  // bit i: pair i of the chunk found no state
     const uint32_t tid = threadIdx.x, W = d.words;
     if (tid == 0) {
         s_count = 1;  // the start set, key index 0, written by the host
@@ -147,39 +148,45 @@ __global__ void __launch_bounds__(DFA_BLOCK) k_dfa_build(DfaDev d) {
         const uint64_t pairs_end = (uint64_t)hi * 64;
         for (uint64_t base = (uint64_t)lo * 64; base < pairs_end && !s_over; base += DFA_CHUNK) {
             const uint32_t cnt = pairs_end - base < DFA_CHUNK ? (uint32_t)(pairs_end - base) : DFA_CHUNK;
+            for (uint32_t w = tid; w < DFA_CHUNK / 32; w += DFA_BLOCK) s_new[w] = 0;
+            __syncthreads();
             for (uint32_t i = tid; i < cnt; i += DFA_BLOCK) {
                 const uint32_t k = (uint32_t)((base + i) >> 6), v = (uint32_t)((base + i) & 63);
                 uint32_t* out = d.cand + (size_t)i * (W + 1);
                 int32_t id = dfa_step(d, k, v, out);
                 if (id < 0) id = dfa_find(d, out);
-                d.cand_id[i] = id;
+                s_id[i] = id;
+                if (id < 0) atomicOr(&s_new[i >> 5], 1u << (i & 31));
             }
             __syncthreads();
-            // new sets get their numbers in (state, value) order
+            // new sets get their numbers in (state, value) order: the set bits of s_new, word by
+            // word, lowest bit first
             if (tid == 0) {
-                for (uint32_t i = 0; i < cnt; i++) {
-                    if (d.cand_id[i] >= 0) continue;
-                    const uint32_t* out = d.cand + (size_t)i * (W + 1);
-                    int32_t id = dfa_find(d, out);
-                    if (id < 0) {
-                        if (s_count + 2 > d.max_states) {
-                            s_over = 1;
-                            break;
+                for (uint32_t wi = 0; wi < (cnt + 31) / 32 && !s_over; wi++) {
+                    for (uint32_t bits = s_new[wi]; bits; bits &= bits - 1) {
+                        const uint32_t i = wi * 32 + __ffs(bits) - 1;
+                        const uint32_t* out = d.cand + (size_t)i * (W + 1);
+                        int32_t id = dfa_find(d, out);
+                        if (id < 0) {
+                            if (s_count + 2 > d.max_states) {
+                                s_over = 1;
+                                break;
+                            }
+                            uint32_t* dst = d.keys + (size_t)s_count * (W + 1);
+                            for (uint32_t j = 0; j <= W; j++) dst[j] = out[j];
+                            dfa_insert(d, s_count);
+                            s_count++;
+                            id = (int32_t)s_count;
                         }
-                        uint32_t* dst = d.keys + (size_t)s_count * (W + 1);
-                        for (uint32_t j = 0; j <= W; j++) dst[j] = out[j];
-                        dfa_insert(d, s_count);
-                        s_count++;
-                        id = (int32_t)s_count;
+                        s_id[i] = id;
                     }
-                    d.cand_id[i] = id;
                 }
             }
             __syncthreads();
             if (!s_over)
                 for (uint32_t i = tid; i < cnt; i += DFA_BLOCK) {
                     const uint32_t k = (uint32_t)((base + i) >> 6), v = (uint32_t)((base + i) & 63);
-                    d.table[(size_t)(k + 1) * 65 + v] = (uint16_t)d.cand_id[i];
+                    d.table[(size_t)(k + 1) * 65 + v] = (uint16_t)s_id[i];
                 }
             __syncthreads();
         }
@@ -213,7 +220,7 @@ cudaError_t build_dfa_device(const mkre::NfaTables& t, uint32_t max_states, cuda
                  o_decm = take(4 * 8 * W), o_endm = take(4 * 4 * W), o_symto = take(4 * n), o_sym = take(8 * n);
     const size_t in_bytes = off;
     const size_t o_keys = take(4 * (size_t)max_states * (W + 1)), o_cand = take(4 * (size_t)DFA_CHUNK * (W + 1)),
-                 o_cid = take(4 * (size_t)DFA_CHUNK), o_hash = take(4 * (size_t)hash_slots),
+                 o_hash = take(4 * (size_t)hash_slots),
                  o_table = take(2 * (size_t)max_states * 65), o_res = take(8);
     std::vector<uint8_t> in(in_bytes, 0);
     auto put = [&](size_t at, const void* src, size_t bytes) {
@@ -254,7 +261,6 @@ cudaError_t build_dfa_device(const mkre::NfaTables& t, uint32_t max_states, cuda
     d.sym = (const uint64_t*)(base + o_sym);
     d.keys = (uint32_t*)(base + o_keys);
     d.cand = (uint32_t*)(base + o_cand);
-    d.cand_id = (int32_t*)(base + o_cid);
     d.hash = (uint32_t*)(base + o_hash);
     d.table = (uint16_t*)(base + o_table);
     d.result = (uint32_t*)(base + o_res);
