@@ -449,6 +449,15 @@ MK_API int mk_openssh_private(const uint8_t seed[32], const char* comment, uint3
 /* Comb table entry (row, column) as 24 words (y+x, y-x, 2dxy; row 0 holds 2xy), for tests. */
 MK_API int mk_table_entry(mk_ctx* ctx, uint32_t row, uint64_t col, uint32_t out[24]);
 
+/* Field products on the device, for tests: for i < n (at most 2^20), a[8i..8i+8) times
+ * b[8i..8i+8) mod 2^255 - 19, little-endian 32-bit words of any value below 2^256, in the
+ * schoolbook form into schoolbook[8i..] and in the Karatsuba form the secure path uses into
+ * karatsuba[8i..].  The results are the kernels' own words: below 2^256, congruent to the
+ * product, not reduced to canonical.  Allocates device memory and waits for the context's
+ * stream. */
+MK_API int mk_field_mul_pairs(mk_ctx* ctx, const uint32_t* a, const uint32_t* b, uint32_t n, uint32_t* schoolbook,
+                              uint32_t* karatsuba);
+
 /* Bytes the job has copied host->device and device->host so far (kernel parameters,
  * compiled needles, job state and hit records), for end-to-end accounting. */
 MK_API int mk_job_io_bytes(const mk_job* job, uint64_t* h2d, uint64_t* d2h);

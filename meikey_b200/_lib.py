@@ -168,6 +168,8 @@ SIGNATURES = [
                                             ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
     ("mk_measure_field_mul_forms", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
                                                   ctypes.POINTER(ctypes.c_double)]),
+    ("mk_field_mul_pairs", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32,
+                                          ctypes.c_void_p, ctypes.c_void_p]),
     ("mk_job_stop", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     ("mk_job_collect", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_uint64)]),
     ("mk_job_first_matches", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(OutcomeC), ctypes.c_uint32]),

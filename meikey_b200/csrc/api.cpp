@@ -1174,6 +1174,14 @@ int mk_regex_compile_device(mk_ctx* c, const char* pattern, int case_sensitive, 
     return MK_OK;
 } MK_ABI_CATCH(c ? &c->err : nullptr)
 
+int mk_field_mul_pairs(mk_ctx* c, const uint32_t* a, const uint32_t* b, uint32_t n, uint32_t* schoolbook,
+                       uint32_t* karatsuba) try {
+    if (!c || !a || !b || !schoolbook || !karatsuba || n == 0 || n > (1u << 20)) return MK_ERR_BAD_ARG;
+    MK_CUDA(c, cudaSetDevice(c->device));
+    MK_CUDA(c, mkb::field_mul_pairs(a, b, n, schoolbook, karatsuba, c->stream));
+    return MK_OK;
+} MK_ABI_CATCH(c ? &c->err : nullptr)
+
 int mk_measure_field_mul_forms(mk_ctx* c, double* schoolbook_per_s, double* karatsuba_per_s) try {
     if (!c || !schoolbook_per_s || !karatsuba_per_s) return MK_ERR_BAD_ARG;
     MK_CUDA(c, cudaSetDevice(c->device));

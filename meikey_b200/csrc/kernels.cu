@@ -1523,6 +1523,40 @@ cudaError_t measure_field_mul_rates(int sms, cudaStream_t st, double* radix32_pe
     return e;
 }
 
+// Products of operand pairs in both radix-2^32 forms: the words (below 2^256, not reduced
+// to canonical) of a[i]·b[i] mod p, schoolbook into out_s and Karatsuba into out_k.
+__global__ void k_fe_mul_pairs(const uint32_t* a, const uint32_t* b, uint32_t n, uint32_t* out_s, uint32_t* out_k) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const mk32::fe x = mk32::fe_from_words(a + (size_t)i * 8), y = mk32::fe_from_words(b + (size_t)i * 8);
+    const mk32::fe s = mk32::fe_mul_schoolbook(x, y), k = mk32::fe_mul_karatsuba(x, y);
+#pragma unroll
+    for (int w = 0; w < 8; w++) {
+        out_s[(size_t)i * 8 + w] = s.v[w];
+        out_k[(size_t)i * 8 + w] = k.v[w];
+    }
+}
+
+cudaError_t field_mul_pairs(const uint32_t* a, const uint32_t* b, uint32_t n, uint32_t* out_s, uint32_t* out_k,
+                            cudaStream_t st) {
+    const size_t bytes = (size_t)n * 32;
+    uint32_t* d = nullptr;
+    cudaError_t e = cudaMalloc(&d, bytes * 4);
+    if (e != cudaSuccess) return e;
+    e = cudaMemcpyAsync(d, a, bytes, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d + (size_t)n * 8, b, bytes, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) {
+        k_fe_mul_pairs<<<(n + 255) / 256, 256, 0, st>>>(d, d + (size_t)n * 8, n, d + (size_t)n * 16,
+                                                        d + (size_t)n * 24);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out_s, d + (size_t)n * 16, bytes, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out_k, d + (size_t)n * 24, bytes, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    const cudaError_t ef = cudaFree(d);
+    return e != cudaSuccess ? e : ef;
+}
+
 // Rates of the two radix-2^32 multiplication forms (schoolbook and Karatsuba), measured like
 // measure_field_mul_rates, and whether their chains end in the same words.
 cudaError_t measure_field_mul_forms(int sms, cudaStream_t st, double* schoolbook_per_s, double* karatsuba_per_s,

@@ -83,6 +83,10 @@ cudaError_t build_dfa_device(const mkre::NfaTables& t, uint32_t max_states, cuda
 // *same_words tells whether their chains ended in the same words.
 cudaError_t measure_field_mul_forms(int sms, cudaStream_t st, double* schoolbook_per_s, double* karatsuba_per_s,
                                     bool* same_words);
+// a[i]·b[i] mod p (8 words each, below 2^256) in the schoolbook and Karatsuba forms, for tests;
+// synchronizes `st`.
+cudaError_t field_mul_pairs(const uint32_t* a, const uint32_t* b, uint32_t n, uint32_t* out_s, uint32_t* out_k,
+                            cudaStream_t st);
 // Integer multiply-adds of one radix-2^32 field multiplication in each form (products and the
 // fold by 38) and of a squaring; the secure path multiplies in the Karatsuba form.
 constexpr double MADS_MUL_SCHOOLBOOK = 64 + 64 + 16;

@@ -195,6 +195,18 @@ class Context:
                self._lib.mk_measure_field_mul(self._ptr, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
         return a.value, b.value, c.value
 
+    def field_mul_pairs(self, a: Sequence[int], b: Sequence[int]):
+        """(schoolbook, karatsuba) lists of the device's a[i]·b[i] mod p for integers below 2^256,
+        as the kernels leave them (below 2^256, congruent, not canonical): mk_field_mul_pairs."""
+        n = len(a)
+        assert n == len(b) and n > 0
+        ina = (ctypes.c_uint32 * (8 * n))(*[(x >> (32 * w)) & 0xffffffff for x in a for w in range(8)])
+        inb = (ctypes.c_uint32 * (8 * n))(*[(x >> (32 * w)) & 0xffffffff for x in b for w in range(8)])
+        outs, outk = (ctypes.c_uint32 * (8 * n))(), (ctypes.c_uint32 * (8 * n))()
+        _check(self._lib, self._ptr, self._lib.mk_field_mul_pairs(self._ptr, ina, inb, n, outs, outk))
+        val = lambda arr, i: sum(arr[8 * i + w] << (32 * w) for w in range(8))
+        return [val(outs, i) for i in range(n)], [val(outk, i) for i in range(n)]
+
     def measure_field_mul_forms(self):
         """{"schoolbook": ..., "karatsuba": ...} radix-2^32 field multiplications per second;
         raises if the two forms' products differ."""

@@ -663,3 +663,23 @@ def test_regex_dialect_over_golden_keys(gpu_ctx, golden, oracle, pattern):
     assert total == len(hits)
     assert [i for i, _ in hits if lo <= i < hi] == want, pattern
     assert want  # every pattern has candidates among these keys
+
+
+def test_field_mul_forms_on_edge_operands(gpu_ctx):
+    """Both radix-2^32 multiplication forms on operands that stress the Karatsuba differences
+    (equal halves, halves differing in sign either way, zero, all-ones limbs, p and its
+    multiples below 2^256) and on random values: the kernels' words are the same in both
+    forms, below 2^256 and congruent to a·b mod p (Python integers)."""
+    import random
+    p = 2**255 - 19
+    h = 2**128
+    edge = [0, 1, 2, 19, 38, p - 1, p, p + 1, 2 * p - 1, 2 * p, 2**255, 2**256 - 1, 2**256 - 38, h - 1, h,
+            (h - 1) * h, (h - 1) * h + (h - 1), 5 * h + 5, 7 * h + 3, 3 * h + 7, (h - 2) * h + (h - 1),
+            (h - 1) * h + (h - 2), 0xffffffff * (h + 1), 2**224 + 2**96]
+    rng = random.Random(11)
+    a = [x for x in edge for _ in edge] + [rng.getrandbits(256) for _ in range(4096)]
+    b = [y for _ in edge for y in edge] + [rng.getrandbits(256) for _ in range(4096)]
+    school, kara = gpu_ctx.field_mul_pairs(a, b)
+    assert school == kara
+    for x, y, r in zip(a, b, school):
+        assert r < 2**256 and r % p == x * y % p
