@@ -293,6 +293,26 @@ def test_incremental_search_matches_oracle(gpu_ctx, oracle):
     assert lowest == min(want0 + want1)
 
 
+GROUP_ORDER = 2**252 + 27742317777372353535851937790883648493
+
+
+@pytest.mark.parametrize("s0", [0, 1, GROUP_ORDER - 5, GROUP_ORDER, 2**255 - 10, 2**255 - 1])
+def test_incremental_edge_start_scalars(gpu_ctx, oracle, s0):
+    """Start scalars at the edges the incremental source allows: zero (the first point is the
+    identity), one, around the group order (s0 + k passes a multiple of it, where the point is
+    the identity again) and just below 2^255 (s0 + k passes 2^255).  Derived keys and one
+    search launch against the oracle's (s0 + k)·B."""
+    key = s0.to_bytes(32, "little")
+    for first, n in ((0, 64), (2**40 + 3, 33)):
+        assert gpu_ctx.derive(key, mk.SEED_INCREMENTAL, first, n) == oracle.derive(key, 2, first, n)
+    kpi = gpu_ctx.keys_per_iter
+    with gpu_ctx.job(key, mk.SEED_INCREMENTAL, [mk.Needle.contains("ab", case_sensitive=False)]) as job:
+        job.launch(0, 1)
+        hits, total = job.hits(cap=1 << 18)
+    assert total == len(hits)
+    assert [i for i, k in hits] == oracle.search(key, 2, 0, kpi, b"ab", 2, True, 0)
+
+
 def test_incremental_rejects_large_start(gpu_ctx):
     """The start scalar must be below 2^255 (s0 + k then never wraps)."""
     bad = bytes(31) + b"\x80"
